@@ -1,0 +1,168 @@
+/*
+ * tgtp_gpu.h — C ABI of the B200 (sm_100a) implementation of the tgtp hot path:
+ * the TGT+ approximate edge spanning centrality tgtp() and the SABA walk counter.
+ *
+ * Every entry point takes plain pointers and sizes, returns a tgtp_status (0 = success) and never
+ * throws.  Host buffers are owned by the caller; the library never keeps a host pointer after a
+ * call returns.  A graph handle owns one CUDA stream (or borrows the caller's, see
+ * tgtp_graph_set_stream); calls on one handle must not run concurrently from several threads.
+ * On failure tgtp_last_error() returns a message for the calling thread.
+ *
+ * Reference interfaces replaced (paths within ggokturk/tgtp):
+ *   fuser::graph_t::load_txt            src/graph.h:29-97      -> tgtp_load_graph_txt + tgtp_graph_upload
+ *   EigenVecs<float>::load_txt          src/aesc.h:51-64       -> tgtp_load_eigens_txt + tgtp_eigens_upload
+ *   AESCGraph(graph, eigens, omega)     src/aesc.h:85-92       -> tgtp_graph_upload + tgtp_eigens_upload
+ *   AESCConfig{epsilon,delta,omega,gamma} src/aesc.h:98-102    -> tgtp_config
+ *   float* AESC::tgtp()                 src/aesc.h:120-127     -> tgtp_run / tgtp_run_device
+ *   saba_randomwalk + runner reduction  src/rw_experiment_saba.cpp:65-145,186-208 -> saba_count
+ *   AESCGraph::free / graph_t::free     src/aesc.h:93-96, src/graph.h:22-28 -> tgtp_graph_free
+ *   exception -> "tgtp: msg", exit 1    src/main.cpp:46-49     -> tgtp_status + tgtp_last_error
+ */
+#ifndef TGTP_GPU_H
+#define TGTP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TGTP_ABI_VERSION 1
+
+typedef enum {
+    TGTP_OK = 0,
+    TGTP_ERR_INVALID_ARGUMENT = 1, /* bad sizes, omega, epsilon, gamma, isolated vertex, ...     */
+    TGTP_ERR_CUDA = 2,             /* a CUDA runtime call or kernel launch failed                */
+    TGTP_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed                           */
+    TGTP_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up (error flag set)        */
+    TGTP_ERR_IO = 5,               /* file could not be opened, parsed or written                */
+    TGTP_ERR_UNSUPPORTED = 6,      /* configuration outside what this build supports             */
+    TGTP_ERR_OVERFLOW = 7          /* a result exceeded its integer type (e.g. a uint32 counter) */
+} tgtp_status;
+
+/* Storage type of eigenvectors on the device. */
+typedef enum {
+    TGTP_VEC_F32 = 0,  /* the reference's own storage (EigenVecs<float>) */
+    TGTP_VEC_F64 = 1,
+    TGTP_VEC_BF16 = 2
+} tgtp_vec_dtype;
+
+/* Arithmetic form of tgtp_run. */
+typedef enum {
+    /* The reference's arithmetic: FP32 residuals/eigenvectors, FP64 logs, the reference's
+     * evaluation order everywhere.  Bit-exact with the reference built at -O2. Needs F32 vectors. */
+    TGTP_PRECISION_FP32 = 0,
+    /* Every float of the reference held in double (needs F64 vectors). */
+    TGTP_PRECISION_FP64 = 1,
+    /* FP32 residuals, lane-parallel compensated FP32 eigen projections over F32 or BF16 vectors,
+     * FP64 tau bounds, stop test and per-edge score accumulation; reductions in parallel order. */
+    TGTP_PRECISION_MIXED = 2
+} tgtp_precision;
+
+typedef struct {
+    double epsilon;    /* 0 < epsilon < 1                                        */
+    double delta;      /* the reference's callers pass 1/n (src/main.cpp:36)      */
+    int32_t omega;     /* number of eigenpairs used, 2 <= omega <= uploaded omega */
+    int32_t gamma;     /* top-gamma residuals for the edge bound, >= 1            */
+    int32_t precision; /* tgtp_precision                                          */
+    int32_t vec_dtype; /* tgtp_vec_dtype read by TGTP_PRECISION_MIXED             */
+} tgtp_config;
+
+typedef struct tgtp_graph tgtp_graph;
+
+/* Work counters of the last tgtp_run on a graph (same meaning as the oracle's counters). */
+typedef struct {
+    uint64_t push_rounds;       /* sum over sources of the final push round count ell   */
+    uint64_t push_vertices;     /* frontier vertices drained                             */
+    uint64_t push_traversals;   /* adjacency entries visited while pushing               */
+    uint64_t walk_edges;        /* CSR slots that ran the 2-way walk                     */
+    uint64_t walk_count;        /* sum of walk counts nr over those slots                */
+    uint64_t walk_hops;         /* sum of nr * remaining length (pairs of hops)          */
+    uint64_t fallback_bouquets; /* bouquets that switched to the SplitMix32 phase        */
+    uint64_t tau_iterations;    /* delta-term evaluations of the tau bound               */
+    uint64_t tau_ambiguous;     /* tau bounds whose ceil() argument lay within 1e-12 of an
+                                   integer (where a last-place libm difference could matter)  */
+} tgtp_run_stats;
+
+typedef struct {
+    uint64_t visit_count;       /* sum of all counters (exact)                            */
+    uint64_t checksum;          /* sum of (v + 1) * counter[v] (exact)                    */
+    uint64_t fallback_bouquets; /* bouquets that switched to the SplitMix32 phase         */
+} saba_result;
+
+/* Per-kernel device time accumulated while profiling is on (tgtp_graph_set_profiling). */
+typedef struct {
+    char name[48];
+    uint64_t launches;
+    double total_ms;
+} tgtp_kernel_stat;
+
+/* ---- errors / version ---------------------------------------------------------------------- */
+const char* tgtp_last_error(void);
+int tgtp_abi_version(void);
+
+/* ---- host-side file loaders (reference file formats) ---------------------------------------- */
+/* graph.txt -> CSR exactly as src/graph.h:29-97 builds it (mirrored edges, rows sorted, no dedup,
+ * n = max id + 1, '#'/'%' comment lines).  *idx (n+1) and *adj (m) are allocated by the library;
+ * release them with tgtp_host_free. */
+tgtp_status tgtp_load_graph_txt(const char* path, uint32_t** idx, uint32_t** adj, uint64_t* n,
+                                uint64_t* m);
+/* sorted_eigens_<omega>.txt -> values[omega] (double) and vertex-major vectors[n*omega], parsed
+ * straight to float (vec_f32) and/or double (vec_f64) as src/aesc.h:51-64 does; either vector
+ * pointer may be NULL.  Caller-allocated buffers. */
+tgtp_status tgtp_load_eigens_txt(const char* path, uint64_t n, uint32_t omega, double* values,
+                                 float* vec_f32, double* vec_f64);
+void tgtp_host_free(void* p);
+
+/* ---- graphs ----------------------------------------------------------------------------------- */
+/* Copies the CSR (host buffers, m = idx[n]) to the current CUDA device.  Rejects m >= 2^32,
+ * non-monotone offsets and out-of-range neighbours. */
+tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint64_t m,
+                              tgtp_graph** out);
+tgtp_status tgtp_graph_free(tgtp_graph* g);
+/* Use the caller's cudaStream_t (NULL: go back to the handle's own stream). */
+tgtp_status tgtp_graph_set_stream(tgtp_graph* g, void* cuda_stream);
+void* tgtp_graph_stream(tgtp_graph* g);
+tgtp_status tgtp_graph_info(const tgtp_graph* g, uint64_t* n, uint64_t* m);
+
+/* Uploads omega eigenpairs (values: double[omega]; vectors: vertex-major n*omega of `dtype`,
+ * F32 or F64 host data).  F64 host data may be stored as F32 or BF16 on the device by passing
+ * the host dtype in `dtype` and the device storage in `store_dtype`.  Several storages may be
+ * uploaded side by side; each call replaces the storage it names. */
+tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* vectors,
+                               uint32_t omega, int32_t dtype, int32_t store_dtype);
+
+/* ---- tgtp ----------------------------------------------------------------------------------- */
+/* Scores of every CSR slot (m float32, symmetric), written to caller-owned host memory.
+ * Synchronous.  AESCConfig validation as src/main.cpp:27-30 and src/aesc.h:87-89. */
+tgtp_status tgtp_run(tgtp_graph* g, const tgtp_config* cfg, float* host_scores);
+/* Same, into caller-owned device memory (m float32), asynchronous on the handle's stream.
+ * Input validation and scratch allocation still happen on the host before the launch. */
+tgtp_status tgtp_run_device(tgtp_graph* g, const tgtp_config* cfg, float* device_scores);
+/* Work counters of the last completed run (synchronises the handle's stream). */
+tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out);
+/* Per-slot tau of the last run (m int32, host). */
+tgtp_status tgtp_last_taus(tgtp_graph* g, int32_t* host_taus);
+
+/* ---- SABA walk counter ---------------------------------------------------------------------- */
+/* n_walks walks of `depth` hops from every vertex with nonzero degree; counters[v] = visits of v
+ * (start vertex excluded).  host_counters (n uint32) may be NULL.  Synchronous.
+ * n_walks must be a multiple of 8 (src/rw_experiment_saba.cpp:160-163). */
+tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* host_counters,
+                       saba_result* out);
+/* Counters into caller-owned device memory (n uint32), asynchronous on the handle's stream. */
+tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
+                              uint32_t* device_counters);
+
+/* ---- profiling ------------------------------------------------------------------------------ */
+/* When on, every kernel launch is bracketed by CUDA events on the handle's stream and its device
+ * time is accumulated per kernel name.  Turning it on clears the table. */
+tgtp_status tgtp_graph_set_profiling(tgtp_graph* g, int enable);
+/* Copies up to `cap` entries; *count = entries available.  Synchronises the stream. */
+tgtp_status tgtp_graph_kernel_stats(tgtp_graph* g, tgtp_kernel_stat* out, int32_t cap,
+                                    int32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TGTP_GPU_H */

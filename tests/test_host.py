@@ -1,0 +1,135 @@
+"""Host side of the library on the CPU: the C ABI loads and exports every entry point the header
+declares; the graph and eigen readers reproduce the reference's loaders (golden dumps from
+src/graph.h and src/aesc.h); the synthetic generators are deterministic simple graphs."""
+from __future__ import annotations
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+
+def _declared_functions():
+    text = open(os.path.join(ROOT, "include", "tgtp_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tgtp_\w+|saba_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(tgtp_lib):
+    from tgtp_b200 import _lib
+
+    names = _declared_functions()
+    assert len(names) >= 19
+    for name in names:
+        assert hasattr(tgtp_lib, name), name
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+    assert tgtp_lib.tgtp_abi_version() == 1
+
+
+@pytest.mark.parametrize("case", ["comments", "selfloop_dup", "isolated_gap", "unsorted",
+                                  "bad_negative", "bad_single", "bad_text", "empty"])
+def test_graph_loader_matches_reference_loader(manifest, tgtp_lib, case):
+    from tgtp_b200.aesc import TgtpError, load_graph_txt
+
+    entry = [e for e in manifest["loader"] if e["case"] == case][0]
+    path = os.path.join(GOLDEN, "loader", entry["file"])
+    if entry["ok"]:
+        idx, adj = load_graph_txt(path)
+        want = np.load(os.path.join(GOLDEN, "loader", entry["csr"]))
+        assert np.array_equal(idx, want["idx"]) and np.array_equal(adj, want["adj"])
+    else:
+        with pytest.raises(TgtpError) as e:
+            load_graph_txt(path)
+        assert e.value.message == entry["error"].replace("{path}", path)
+
+
+def test_graph_loader_missing_file(tgtp_lib):
+    from tgtp_b200.aesc import TgtpError, load_graph_txt
+
+    with pytest.raises(TgtpError) as e:
+        load_graph_txt("/nonexistent/graph.txt")
+    assert e.value.status == 5 and "cannot open graph" in e.value.message
+
+
+def test_eigen_loader_matches_reference_loader(manifest, tgtp_lib):
+    from tgtp_b200.aesc import load_eigens_txt
+
+    e = manifest["eigens"][0]
+    folder = os.path.join(GOLDEN, "eigens")
+    vals, v32, v64 = load_eigens_txt(os.path.join(folder, e["eigens"]), e["n"], e["omega"])
+    want = np.load(os.path.join(folder, e["parsed"]))
+    assert np.array_equal(vals, want["values"])
+    assert np.array_equal(v32.view(np.uint32), want["vectors"].view(np.uint32))
+
+
+def test_eigen_loader_rejects_short_and_nonfinite(tmp_path, tgtp_lib):
+    from tgtp_b200.aesc import TgtpError, load_eigens_txt
+
+    p = tmp_path / "e.txt"
+    p.write_text("1 0.5 0.5\n")
+    with pytest.raises(TgtpError):
+        load_eigens_txt(str(p), 2, 2)
+    p.write_text("1 0.5 nan\n0.5 1 1\n")
+    with pytest.raises(TgtpError):
+        load_eigens_txt(str(p), 2, 2)
+
+
+def test_eigen_loader_agrees_with_oracle_parser_on_golden_files(manifest, tgtp_lib, oracle_lib):
+    from tgtp_b200.aesc import load_eigens_txt
+
+    for case in {r["case"]: r for r in manifest["tgtp"]}.values():
+        path = os.path.join(GOLDEN, "tgtp", case["case"], f"sorted_eigens_{case['omega']}.txt")
+        a = load_eigens_txt(path, case["n"], case["omega"])
+        b = oracle_lib.parse_eigens(path, case["n"], case["omega"])
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+
+
+def test_synthetic_generators_are_seeded_simple_connected():
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    from tgtp_b200 import synth
+
+    for make in (lambda s: synth.chung_lu(500, 3000, 2.3, s),
+                 lambda s: synth.rmat(9, 8, 0.57, 0.19, 0.19, s),
+                 lambda s: synth.grid_chords(12, 15, 6.0, s)):
+        g1, g2, g3 = make(1), make(1), make(2)
+        assert np.array_equal(g1.u, g2.u) and np.array_equal(g1.v, g2.v)
+        assert not (np.array_equal(g1.u, g3.u) and np.array_equal(g1.v, g3.v))
+        assert np.all(g1.u < g1.v)
+        key = g1.u * g1.n + g1.v
+        assert np.unique(key).size == key.size
+        a = coo_matrix((np.ones(g1.num_edges), (g1.u, g1.v)), shape=(g1.n, g1.n))
+        assert connected_components(a, directed=False)[0] == 1
+        idx, adj = g1.csr()
+        assert idx[-1] == 2 * g1.num_edges and np.all(np.diff(idx.astype(np.int64)) > 0)
+
+
+def test_config1_graph_shape():
+    from tgtp_b200 import synth
+
+    g = synth.config1_graph(1)
+    assert g.n == 4039 and g.num_edges == 88234
+
+
+def test_eigenprep_pairs_are_eigenpairs_of_the_random_walk_matrix(tmp_path):
+    """x = D^-1/2 v * sqrt(2m) for A_hat v = lambda v  <=>  D^-1 A x = lambda x."""
+    from tgtp_b200 import eigenprep, synth
+
+    g = synth.chung_lu(200, 1200, 2.5, 3)
+    synth.write_graph_txt(g, str(tmp_path / "graph.txt"))
+    path = eigenprep.eigenprep_folder(str(tmp_path), 12)
+    rows = np.loadtxt(path)
+    vals, vecs = rows[:, 0], rows[:, 1:]
+    idx, adj = g.csr()
+    deg = np.diff(idx.astype(np.int64))
+    assert np.all(np.diff(np.abs(vals)) <= 1e-12)
+    assert abs(vals[0] - 1) < 1e-8
+    for lam, x in zip(vals, vecs):
+        ax = np.add.reduceat(x[adj], idx[:-1]) / deg
+        assert np.max(np.abs(ax - lam * x)) < 1e-5 * np.max(np.abs(x))
+    assert (tmp_path / "stat.txt").read_text().startswith("n=200\nm=")

@@ -1,0 +1,93 @@
+"""SABA walk counter on the GPU, through the C ABI: counters bit-exact with the reference's golden
+vectors and with the oracle at larger sizes; visit_count = active vertices * W * D exactly."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(path):
+    from tgtp_b200.aesc import AESCGraph
+
+    return AESCGraph(path)
+
+
+def test_saba_matches_reference_golden(manifest, cuda_device):
+    from tgtp_b200.aesc import saba_count
+
+    for run in manifest["saba"]:
+        g = _graph(os.path.join(GOLDEN, "saba", run["graph"]))
+        counts, visits, checksum, _ = saba_count(g, run["depth"], run["n_walks"])
+        want = np.load(os.path.join(GOLDEN, "saba", run["counts"]))
+        assert np.array_equal(counts, want), run
+        assert visits == run["visit_count"] and checksum == run["checksum"]
+        g.free()
+
+
+@pytest.mark.parametrize("depth,walks", [(5, 2048), (10, 64), (15, 16)])
+def test_saba_config1_graph_matches_oracle(cuda_device, oracle_lib, depth, walks):
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    g = synth.config1_graph(1)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, checksum, fb = saba_count(dg, depth, walks)
+    want = oracle_lib.saba(idx, adj, depth, walks)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    assert visits == g.n * walks * depth
+    assert checksum == int((want * np.arange(1, g.n + 1, dtype=np.uint64)).sum())
+    dg.free()
+
+
+def test_saba_rmat_beyond_shared_counters_matches_oracle(cuda_device, oracle_lib):
+    """n above the shared-memory counter range: hot ids in shared memory, the rest in L2."""
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    g = synth.rmat(15, 8, 0.57, 0.19, 0.19, 9)
+    idx, adj = g.csr()
+    assert g.n > 12288
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, _, _ = saba_count(dg, 7, 32)
+    want = oracle_lib.saba(idx, adj, 7, 32)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    assert visits == g.n * 32 * 7
+    dg.free()
+
+
+def test_saba_fallback_phase_is_exercised(cuda_device, oracle_lib):
+    """16-regular graph: secrets hit zero after 8 hops and the SplitMix32 phase takes over."""
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    run = [r for r in [dict(graph="circ16.graph.txt", depth=10, n_walks=64)]][0]
+    g = _graph(os.path.join(GOLDEN, "saba", run["graph"]))
+    _, _, _, fb = saba_count(g, run["depth"], run["n_walks"], counters=False)
+    assert fb == g.n * run["n_walks"] // 8
+    g.free()
+
+
+def test_saba_rejects_partial_bouquets(cuda_device):
+    from tgtp_b200.aesc import TgtpError, saba_count
+
+    g = _graph(os.path.join(GOLDEN, "saba", "cl300.graph.txt"))
+    with pytest.raises(TgtpError) as e:
+        saba_count(g, 5, 12)
+    assert "multiple of 8" in str(e.value)
+    g.free()
+
+
+def test_saba_zero_walks_and_zero_depth(cuda_device):
+    from tgtp_b200.aesc import saba_count
+
+    g = _graph(os.path.join(GOLDEN, "saba", "cl300.graph.txt"))
+    for d, w in ((0, 64), (5, 0)):
+        counts, visits, checksum, _ = saba_count(g, d, w)
+        assert visits == 0 and checksum == 0 and not counts.any()
+    g.free()

@@ -1,0 +1,146 @@
+"""tgtp() on the GPU, through the C ABI.
+
+FP32 form: bit-exact with the reference (golden vectors) and with the oracle.
+FP64 form: bit-exact with the oracle's FP64 restatement (same operations, same order) and within
+           1e-6 relative (or 2 float32 ulps) of the reference on all but <= 1% of slots.
+Work counters (push rounds, traversals, walks, fallbacks) equal the oracle's."""
+from __future__ import annotations
+
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import golden_tgtp_case, load_golden_scores
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12"]
+STAT_KEYS = ["push_rounds", "push_vertices", "push_traversals", "walk_edges", "walk_count",
+             "walk_hops", "fallback_bouquets", "tau_iterations"]
+
+
+def _device_graph(c, fp64=False):
+    from tgtp_b200.aesc import VEC_F32, VEC_F64, AESCGraph
+
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    if fp64:
+        g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    return g
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_bit_exact_with_reference(manifest, cuda_device, name):
+    from tgtp_b200.aesc import AESC, AESCConfig
+
+    c = golden_tgtp_case(manifest, name)
+    g = _device_graph(c)
+    for run in c["runs"]:
+        a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"]))
+        got = a.tgtp()
+        want = load_golden_scores(run)
+        bad = np.flatnonzero(got.view(np.uint32) != want.view(np.uint32))
+        assert bad.size == 0, (run, bad[:8], got[bad[:4]], want[bad[:4]])
+        assert a.stats()["tau_ambiguous"] == 0
+    g.free()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_taus_and_work_counters_match_oracle(manifest, cuda_device, oracle_lib, name):
+    from tgtp_b200.aesc import AESC, AESCConfig
+
+    c = golden_tgtp_case(manifest, name)
+    g = _device_graph(c)
+    for run in c["runs"]:
+        a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"]))
+        a.tgtp()
+        _, det = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v32"], run["epsilon"],
+                                 gamma=run["gamma"], details=True)
+        assert np.array_equal(a.taus(), det["taus"])
+        st = a.stats()
+        for k in STAT_KEYS:
+            assert st[k] == det["stats"][k], (run, k, st[k], det["stats"][k])
+    g.free()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_oracle_and_reference(manifest, cuda_device, oracle_lib, name):
+    from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_FP64
+
+    c = golden_tgtp_case(manifest, name)
+    g = _device_graph(c, fp64=True)
+    for run in c["runs"]:
+        a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"],
+                               precision=PRECISION_FP64))
+        got = a.tgtp()
+        ora = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], run["epsilon"],
+                              gamma=run["gamma"], fp64=True)
+        assert np.array_equal(got.view(np.uint32), ora.view(np.uint32)), run
+        want = load_golden_scores(run)
+        tol = np.maximum(1e-6 * np.abs(want), 2 * np.spacing(np.abs(want)))
+        assert (np.abs(got.astype(np.float64) - want) > tol).mean() <= 0.01
+    g.free()
+
+
+@pytest.fixture(scope="module")
+def config1_inputs():
+    """Chung-Lu n=4,039 with 128 eigenpairs written and parsed back like the reference's files."""
+    from tgtp_b200 import eigenprep, synth
+    from tgtp_b200.aesc import load_eigens_txt
+
+    g = synth.config1_graph(1)
+    d = tempfile.mkdtemp(prefix="tgtp_cfg1_")
+    synth.write_graph_txt(g, os.path.join(d, "graph.txt"))
+    path = eigenprep.eigenprep_folder(d, 128)
+    idx, adj = g.csr()
+    values, v32, v64 = load_eigens_txt(path, g.n, 128)
+    return dict(idx=idx, adj=adj, values=values, v32=v32, v64=v64, n=g.n)
+
+
+@pytest.mark.parametrize("eps", [0.05, 0.01, 0.005])
+def test_config1_fp32_bit_exact_with_oracle(cuda_device, oracle_lib, config1_inputs, eps):
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, VEC_F32
+
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    got = AESC(g, AESCConfig(eps)).tgtp()
+    want = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v32"], eps)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    g.free()
+
+
+def test_config1_fp64_bit_exact_with_oracle(cuda_device, oracle_lib, config1_inputs):
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, PRECISION_FP64, VEC_F64
+
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    got = AESC(g, AESCConfig(0.05, precision=PRECISION_FP64)).tgtp()
+    want = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], 0.05, fp64=True)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    g.free()
+
+
+def test_invalid_arguments_are_rejected(manifest, cuda_device):
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, TgtpError, PRECISION_FP64
+
+    c = golden_tgtp_case(manifest, "cl300")
+    g = _device_graph(c)
+    for cfg in (AESCConfig(0.0, omega=16), AESCConfig(1.0, omega=16),
+                AESCConfig(0.05, omega=16, gamma=0), AESCConfig(0.05, omega=1),
+                AESCConfig(0.05, omega=32), AESCConfig(0.05, omega=16, precision=PRECISION_FP64)):
+        with pytest.raises(TgtpError) as e:
+            AESC(g, cfg).tgtp()
+        assert e.value.status == 1, cfg
+    g.free()
+    # isolated vertex: AESCGraph rejects it (src/aesc.h:88-89)
+    idx = np.array([0, 1, 2, 2, 2], np.uint32)
+    adj = np.array([1, 0], np.uint32)
+    g = AESCGraph.from_csr(idx, adj)
+    with pytest.raises(TgtpError):
+        g.upload_eigens(np.array([1.0, 0.5]), np.zeros(8, np.float32))
+        AESC(g, AESCConfig(0.05, omega=2)).tgtp()
+    g.free()

@@ -1,0 +1,484 @@
+// C ABI of libtgtp_gpu (include/tgtp_gpu.h): graph/eigen upload, device-side preparation of the
+// per-slot maps, the SABA entry points, profiling, and error reporting.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace tgtp {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// ---- profiler ------------------------------------------------------------------------------------
+cudaEvent_t Profiler::take() {
+    if (!pool_.empty()) {
+        cudaEvent_t e = pool_.back();
+        pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    TGTP_CUDA(cudaEventCreate(&e));
+    return e;
+}
+void Profiler::begin(cudaStream_t s, const char* name) {
+    open_ = take();
+    open_name_ = name;
+    TGTP_CUDA(cudaEventRecord(open_, s));
+}
+void Profiler::end(cudaStream_t s) {
+    if (!open_) return;
+    cudaEvent_t b = take();
+    if (cudaEventRecord(b, s) != cudaSuccess) return;  // called from a destructor: never throw
+    pending_.push_back({open_name_, open_, b});
+    open_ = nullptr;
+}
+void Profiler::collect() {
+    for (auto& p : pending_) {
+        TGTP_CUDA(cudaEventSynchronize(p.b));
+        float ms = 0;
+        TGTP_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        auto it = std::find_if(totals.begin(), totals.end(),
+                               [&](const Entry& e) { return e.name == p.name; });
+        if (it == totals.end()) {
+            totals.push_back({p.name, 0, 0});
+            it = totals.end() - 1;
+        }
+        it->launches += 1;
+        it->total_ms += ms;
+        pool_.push_back(p.a);
+        pool_.push_back(p.b);
+    }
+    pending_.clear();
+}
+void Profiler::clear() {
+    for (auto& p : pending_) {
+        cudaEventSynchronize(p.b);
+        pool_.push_back(p.a);
+        pool_.push_back(p.b);
+    }
+    pending_.clear();
+    totals.clear();
+}
+Profiler::~Profiler() {
+    for (auto& p : pending_) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : pool_) cudaEventDestroy(e);
+}
+
+// ---- per-slot maps built on the device at upload -----------------------------------------------
+namespace {
+
+__global__ void degree_kernel(const uint32_t* __restrict__ idx, uint64_t n, uint32_t* __restrict__ deg) {
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+         v += uint64_t(gridDim.x) * blockDim.x)
+        deg[v] = idx[v + 1] - idx[v];
+}
+
+// row_of[pos] = u with idx[u] <= pos < idx[u+1] (rows may be empty: take the last such u).
+__global__ void row_of_kernel(const uint32_t* __restrict__ idx, uint64_t n, uint64_t m,
+                              uint32_t* __restrict__ row_of) {
+    for (uint64_t pos = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; pos < m;
+         pos += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t lo = 0, hi = n;  // largest u with idx[u] <= pos
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (idx[mid] <= pos) lo = mid;
+            else hi = mid;
+        }
+        row_of[pos] = uint32_t(lo);
+    }
+}
+
+// rev[pos] = lower_bound(row v, u) for slot (u, v): the slot src/aesc.h:207-209 and :541-542 address.
+// sym_src[q] = 1 + max{pos : rev[pos] == q}: the slot whose value lands in rev_preds[q] last
+// (src/aesc.h:538-545 writes rows in order, so the largest pos wins).
+__global__ void rev_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
+                           const uint32_t* __restrict__ row_of, uint64_t m,
+                           uint32_t* __restrict__ rev, uint32_t* __restrict__ sym_src) {
+    for (uint64_t pos = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; pos < m;
+         pos += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t u = row_of[pos], v = adj[pos];
+        const uint32_t q = lower_bound_u32(adj, idx[v], idx[v + 1], u);
+        rev[pos] = q;
+        atomicMax(sym_src + q, uint32_t(pos + 1));
+    }
+}
+
+// forward slots (v >= u) are the tail of each sorted row; count them per row.
+__global__ void forward_count_kernel(const uint32_t* __restrict__ idx,
+                                     const uint32_t* __restrict__ adj, uint64_t n,
+                                     uint32_t* __restrict__ cnt) {
+    for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < n;
+         u += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t lb = lower_bound_u32(adj, idx[u], idx[u + 1], uint32_t(u));
+        cnt[u] = idx[u + 1] - lb;
+    }
+}
+
+// Exclusive scan of cnt[0..n) in one block, chunk by chunk with a running carry; writes the total
+// to cnt_total.  Runs once per upload.
+__global__ void scan_kernel(uint32_t* __restrict__ cnt, uint64_t n, uint32_t* __restrict__ total) {
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint64_t base = 0; base < n; base += blockDim.x) {
+        const uint64_t i = base + threadIdx.x;
+        const uint32_t x = i < n ? cnt[i] : 0;
+        uint32_t incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const uint32_t nw = blockDim.x >> 5;
+            uint32_t ws = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFullMask, ws, o);
+                if (lane >= uint32_t(o)) ws += y;
+            }
+            if (lane < nw) warp_sums[lane] = ws;  // inclusive
+        }
+        __syncthreads();
+        const uint32_t before = (wid ? warp_sums[wid - 1] : 0) + carry;
+        if (i < n) cnt[i] = before + incl - x;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = before + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void forward_fill_kernel(const uint32_t* __restrict__ idx,
+                                    const uint32_t* __restrict__ adj, uint64_t n,
+                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ fwd) {
+    for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < n;
+         u += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t lb = lower_bound_u32(adj, idx[u], idx[u + 1], uint32_t(u));
+        const uint32_t o = off[u];
+        for (uint32_t p = lb; p < idx[u + 1]; ++p) fwd[o + (p - lb)] = p;
+    }
+}
+
+__global__ void f64_to_storage_kernel(const double* __restrict__ in, uint64_t count,
+                                      float* __restrict__ out_f32, __nv_bfloat16* __restrict__ out_bf16) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        if (out_f32) out_f32[i] = __double2float_rn(in[i]);
+        if (out_bf16) out_bf16[i] = __double2bfloat16(in[i]);
+    }
+}
+__global__ void f32_to_bf16_kernel(const float* __restrict__ in, uint64_t count,
+                                   __nv_bfloat16* __restrict__ out) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        out[i] = __float2bfloat16_rn(in[i]);
+}
+
+unsigned grid_for(uint64_t work, int num_sms) {
+    const uint64_t b = (work + 255) / 256;
+    const uint64_t cap = uint64_t(num_sms) * 8;
+    return unsigned(std::max<uint64_t>(1, std::min(b, cap)));
+}
+
+}  // namespace
+
+void graph_prepare(tgtp_graph* g) {
+    cudaStream_t s = g->stream;
+    const uint64_t n = g->n, m = g->m;
+    auto* idx = g->idx.as<uint32_t>();
+    auto* adj = g->adj.as<uint32_t>();
+    g->deg.reserve(sizeof(uint32_t) * (n + 1));
+    g->row_of.reserve(sizeof(uint32_t) * (m + 1));
+    g->rev.reserve(sizeof(uint32_t) * (m + 1));
+    g->sym_src.reserve(sizeof(uint32_t) * (m + 1));
+    degree_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, n, g->deg.as<uint32_t>());
+    TGTP_LAUNCH_CHECK("degree_kernel");
+    if (m) {
+        row_of_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(idx, n, m, g->row_of.as<uint32_t>());
+        TGTP_LAUNCH_CHECK("row_of_kernel");
+        TGTP_CUDA(cudaMemsetAsync(g->sym_src.ptr, 0, sizeof(uint32_t) * m, s));
+        rev_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(idx, adj, g->row_of.as<uint32_t>(), m,
+                                                           g->rev.as<uint32_t>(),
+                                                           g->sym_src.as<uint32_t>());
+        TGTP_LAUNCH_CHECK("rev_kernel");
+    }
+    // forward slot list
+    DeviceBuffer cnt;
+    cnt.reserve(sizeof(uint32_t) * (n + 2));
+    auto* c = cnt.as<uint32_t>();
+    forward_count_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c);
+    TGTP_LAUNCH_CHECK("forward_count_kernel");
+    scan_kernel<<<1, 1024, 0, s>>>(c, n, c + n + 1);
+    TGTP_LAUNCH_CHECK("scan_kernel");
+    uint32_t total = 0;
+    TGTP_CUDA(cudaMemcpyAsync(&total, c + n + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TGTP_CUDA(cudaStreamSynchronize(s));
+    g->num_forward = total;
+    g->forward.reserve(sizeof(uint32_t) * (total + 1));
+    forward_fill_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c,
+                                                                g->forward.as<uint32_t>());
+    TGTP_LAUNCH_CHECK("forward_fill_kernel");
+    TGTP_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace tgtp
+
+tgtp_graph::~tgtp_graph() {
+    if (own_stream) {
+        cudaStreamSynchronize(own_stream);
+        cudaStreamDestroy(own_stream);
+    }
+}
+
+using namespace tgtp;
+
+extern "C" {
+
+const char* tgtp_last_error(void) { return g_last_error.c_str(); }
+int tgtp_abi_version(void) { return TGTP_ABI_VERSION; }
+void tgtp_host_free(void* p) { std::free(p); }
+
+tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint64_t m,
+                              tgtp_graph** out) {
+    return guarded([&] {
+        if (!out) fail(TGTP_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        if (!idx || (m && !adj)) fail(TGTP_ERR_INVALID_ARGUMENT, "null CSR pointer");
+        if (n == 0) fail(TGTP_ERR_INVALID_ARGUMENT, "empty graph");
+        if (n >= 0xffffffffull) fail(TGTP_ERR_INVALID_ARGUMENT, "vertex count exceeds uint32");
+        if (m >= 0xffffffffull) fail(TGTP_ERR_INVALID_ARGUMENT, "graph exceeds CSR index capacity");
+        if (idx[0] != 0 || idx[n] != m)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "row offsets must start at 0 and end at m");
+        auto g = std::make_unique<tgtp_graph>();
+        g->n = n;
+        g->m = m;
+        uint32_t maxd = 0, mind = 0xffffffffu;
+        uint64_t active = 0;
+        bool multi = false;
+        for (uint64_t v = 0; v < n; ++v) {
+            if (idx[v + 1] < idx[v]) fail(TGTP_ERR_INVALID_ARGUMENT, "row offsets decrease");
+            const uint32_t d = idx[v + 1] - idx[v];
+            maxd = std::max(maxd, d);
+            mind = std::min(mind, d);
+            active += d != 0;
+            for (uint32_t p = idx[v]; p < idx[v + 1]; ++p) {
+                if (adj[p] >= n) fail(TGTP_ERR_INVALID_ARGUMENT, "neighbour id out of range");
+                if (p > idx[v]) {
+                    if (adj[p] < adj[p - 1]) fail(TGTP_ERR_INVALID_ARGUMENT, "rows must be sorted");
+                    if (adj[p] == adj[p - 1]) multi = true;
+                }
+            }
+        }
+        g->max_degree = maxd;
+        g->min_degree = mind;
+        g->num_active = active;
+        g->has_multi_edges = multi;
+        TGTP_CUDA(cudaGetDevice(&g->device));
+        TGTP_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
+        TGTP_CUDA(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+        g->stream = g->own_stream;
+        g->idx.reserve(sizeof(uint32_t) * (n + 1));
+        g->adj.reserve(sizeof(uint32_t) * (m + 1));
+        TGTP_CUDA(cudaMemcpyAsync(g->idx.ptr, idx, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice,
+                                  g->stream));
+        if (m)
+            TGTP_CUDA(cudaMemcpyAsync(g->adj.ptr, adj, sizeof(uint32_t) * m, cudaMemcpyHostToDevice,
+                                      g->stream));
+        graph_prepare(g.get());
+        *out = g.release();
+    });
+}
+
+tgtp_status tgtp_graph_free(tgtp_graph* g) {
+    return guarded([&] { delete g; });
+}
+
+tgtp_status tgtp_graph_set_stream(tgtp_graph* g, void* cuda_stream) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        TGTP_CUDA(cudaStreamSynchronize(g->stream));
+        g->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : g->own_stream;
+    });
+}
+
+void* tgtp_graph_stream(tgtp_graph* g) { return g ? static_cast<void*>(g->stream) : nullptr; }
+
+tgtp_status tgtp_graph_info(const tgtp_graph* g, uint64_t* n, uint64_t* m) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        if (n) *n = g->n;
+        if (m) *m = g->m;
+    });
+}
+
+tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* vectors,
+                               uint32_t omega, int32_t dtype, int32_t store_dtype) {
+    return guarded([&] {
+        if (!g || !values || !vectors) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
+        if (omega < 2 || omega > g->n)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "omega must be between 2 and vertex count");
+        if (dtype != TGTP_VEC_F32 && dtype != TGTP_VEC_F64)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "host eigenvectors must be F32 or F64");
+        if (store_dtype < TGTP_VEC_F32 || store_dtype > TGTP_VEC_BF16)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "unknown storage dtype");
+        if (dtype == TGTP_VEC_F32 && store_dtype == TGTP_VEC_F64)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "F32 host data cannot be stored as F64");
+        for (uint32_t i = 0; i < omega; ++i)
+            if (!std::isfinite(values[i])) fail(TGTP_ERR_INVALID_ARGUMENT, "invalid eigenvalue");
+        if (g->omega != omega) {
+            g->has_f32 = g->has_f64 = g->has_bf16 = false;
+        }
+        cudaStream_t s = g->stream;
+        const uint64_t count = g->n * uint64_t(omega);
+        g->omega = omega;
+        g->values.assign(values, values + omega);
+        g->d_values.reserve(sizeof(double) * omega);
+        TGTP_CUDA(cudaMemcpyAsync(g->d_values.ptr, values, sizeof(double) * omega,
+                                  cudaMemcpyHostToDevice, s));
+        // tau-bound tables: onep/onem per eigen index, and eigen_t_1 after k multiplications
+        // (src/aesc.h:174-176, :190, :201-203), in the reference's exact sequence of roundings.
+        constexpr int kRows = 64;
+        std::vector<double> onep(omega), onem(omega), tab(size_t(kRows) * omega);
+        std::vector<float> tabf(size_t(kRows) * omega);
+        for (uint32_t i = 0; i < omega; ++i) {
+            onep[i] = 1 + values[i];
+            onem[i] = 1 - values[i];
+            const double sq = values[i] * values[i];
+            double e = sq;
+            for (int k = 0; k < kRows; ++k) {
+                tab[size_t(k) * omega + i] = e;
+                tabf[size_t(k) * omega + i] = float(e);
+                e *= sq;
+            }
+        }
+        g->onep.reserve(sizeof(double) * omega);
+        g->onem.reserve(sizeof(double) * omega);
+        g->etab.reserve(sizeof(double) * tab.size());
+        g->etab_f.reserve(sizeof(float) * tabf.size());
+        TGTP_CUDA(cudaMemcpyAsync(g->onep.ptr, onep.data(), sizeof(double) * omega,
+                                  cudaMemcpyHostToDevice, s));
+        TGTP_CUDA(cudaMemcpyAsync(g->onem.ptr, onem.data(), sizeof(double) * omega,
+                                  cudaMemcpyHostToDevice, s));
+        TGTP_CUDA(cudaMemcpyAsync(g->etab.ptr, tab.data(), sizeof(double) * tab.size(),
+                                  cudaMemcpyHostToDevice, s));
+        TGTP_CUDA(cudaMemcpyAsync(g->etab_f.ptr, tabf.data(), sizeof(float) * tabf.size(),
+                                  cudaMemcpyHostToDevice, s));
+        const unsigned blocks = grid_for(count, g->num_sms);
+        if (dtype == TGTP_VEC_F32) {
+            g->vec_f32.reserve(sizeof(float) * count);
+            TGTP_CUDA(cudaMemcpyAsync(g->vec_f32.ptr, vectors, sizeof(float) * count,
+                                      cudaMemcpyHostToDevice, s));
+            if (store_dtype == TGTP_VEC_BF16) {
+                g->vec_bf16.reserve(sizeof(__nv_bfloat16) * count);
+                f32_to_bf16_kernel<<<blocks, 256, 0, s>>>(g->vec_f32.as<float>(), count,
+                                                          g->vec_bf16.as<__nv_bfloat16>());
+                TGTP_LAUNCH_CHECK("f32_to_bf16_kernel");
+                g->has_bf16 = true;
+            } else {
+                g->has_f32 = true;
+            }
+        } else {
+            g->vec_f64.reserve(sizeof(double) * count);
+            TGTP_CUDA(cudaMemcpyAsync(g->vec_f64.ptr, vectors, sizeof(double) * count,
+                                      cudaMemcpyHostToDevice, s));
+            if (store_dtype == TGTP_VEC_F64) {
+                g->has_f64 = true;
+            } else {
+                float* f32 = nullptr;
+                __nv_bfloat16* b16 = nullptr;
+                if (store_dtype == TGTP_VEC_F32) {
+                    g->vec_f32.reserve(sizeof(float) * count);
+                    f32 = g->vec_f32.as<float>();
+                    g->has_f32 = true;
+                } else {
+                    g->vec_bf16.reserve(sizeof(__nv_bfloat16) * count);
+                    b16 = g->vec_bf16.as<__nv_bfloat16>();
+                    g->has_bf16 = true;
+                }
+                f64_to_storage_kernel<<<blocks, 256, 0, s>>>(g->vec_f64.as<double>(), count, f32, b16);
+                TGTP_LAUNCH_CHECK("f64_to_storage_kernel");
+            }
+        }
+        TGTP_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
+                              uint32_t* device_counters) {
+    return guarded([&] {
+        if (!g || !device_counters) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
+        if (n_walks % 8 != 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "n_walks must be a multiple of 8 within the 32-bit grid domain");
+        saba_run(g, depth, n_walks, device_counters);
+    });
+}
+
+tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* host_counters,
+                       saba_result* out) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        if (n_walks % 8 != 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "n_walks must be a multiple of 8 within the 32-bit grid domain");
+        g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
+        auto* c = g->counters.as<uint32_t>();
+        saba_run(g, depth, n_walks, c);
+        uint64_t sums[3];
+        saba_summarize(g, c, sums);
+        if (host_counters)
+            TGTP_CUDA(cudaMemcpy(host_counters, c, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost));
+        if (out) {
+            out->visit_count = sums[0];
+            out->checksum = sums[1];
+            out->fallback_bouquets = sums[2];
+        }
+        // Every walk makes exactly `depth` hops, so a wrapped uint32 counter shows as a shortfall.
+        const unsigned __int128 expect = (unsigned __int128)g->num_active * n_walks * depth;
+        if ((unsigned __int128)sums[0] != expect)
+            fail(TGTP_ERR_OVERFLOW, "a uint32 visit counter overflowed");
+    });
+}
+
+tgtp_status tgtp_graph_set_profiling(tgtp_graph* g, int enable) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        g->prof.clear();
+        g->prof.enabled = enable != 0;
+    });
+}
+
+tgtp_status tgtp_graph_kernel_stats(tgtp_graph* g, tgtp_kernel_stat* out, int32_t cap,
+                                    int32_t* count) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        g->prof.collect();
+        const auto& t = g->prof.totals;
+        if (count) *count = int32_t(t.size());
+        for (int32_t i = 0; i < cap && i < int32_t(t.size()); ++i) {
+            std::snprintf(out[i].name, sizeof(out[i].name), "%s", t[i].name.c_str());
+            out[i].launches = t[i].launches;
+            out[i].total_ms = t[i].total_ms;
+        }
+    });
+}
+
+}  // extern "C"

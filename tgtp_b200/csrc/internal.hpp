@@ -1,0 +1,173 @@
+// Internal declarations of libtgtp_gpu: error plumbing, device buffers, the graph handle and the
+// per-kernel event profiler.  Nothing here crosses the C ABI (include/tgtp_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "tgtp_gpu.h"
+
+namespace tgtp {
+
+// Internal failures travel as exceptions and are turned into a status at the ABI boundary.
+struct Error {
+    tgtp_status code;
+    std::string msg;
+};
+
+[[noreturn]] inline void fail(tgtp_status code, const std::string& msg) { throw Error{code, msg}; }
+
+void set_last_error(const std::string& msg);
+
+#define TGTP_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            (void)cudaGetLastError();                                                          \
+            ::tgtp::fail(e_ == cudaErrorMemoryAllocation ? TGTP_ERR_OUT_OF_MEMORY : TGTP_ERR_CUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+        }                                                                                      \
+    } while (0)
+
+#define TGTP_LAUNCH_CHECK(name)                                                                \
+    do {                                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess)                                                                 \
+            ::tgtp::fail(TGTP_ERR_CUDA, std::string("launch of ") + (name) + ": " +            \
+                                            cudaGetErrorString(e_));                           \
+    } while (0)
+
+template <class F>
+tgtp_status guarded(F&& f) {
+    try {
+        f();
+        return TGTP_OK;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return TGTP_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return TGTP_ERR_INVALID_ARGUMENT;
+    }
+}
+
+// Grow-only device allocation owned by a graph handle.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void reserve(size_t want) {
+        if (want <= bytes && ptr) return;
+        release();
+        if (want == 0) want = 16;
+        TGTP_CUDA(cudaMalloc(&ptr, want));
+        bytes = want;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// CUDA-event timing of each kernel launch on the handle's stream (off unless asked for).
+class Profiler {
+public:
+    bool enabled = false;
+    void begin(cudaStream_t s, const char* name);
+    void end(cudaStream_t s);
+    void clear();
+    // Synchronises the pending events and folds them into the totals.
+    void collect();
+    struct Entry {
+        std::string name;
+        uint64_t launches = 0;
+        double total_ms = 0;
+    };
+    std::vector<Entry> totals;
+    ~Profiler();
+
+private:
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending_;
+    std::vector<cudaEvent_t> pool_;
+    cudaEvent_t take();
+    const char* open_name_ = nullptr;
+    cudaEvent_t open_ = nullptr;
+};
+
+struct ScopedKernel {
+    Profiler& p;
+    cudaStream_t s;
+    ScopedKernel(Profiler& p_, cudaStream_t s_, const char* name) : p(p_), s(s_) {
+        if (p.enabled) p.begin(s, name);
+    }
+    ~ScopedKernel() {
+        if (p.enabled) p.end(s);
+    }
+};
+
+}  // namespace tgtp
+
+// The opaque handle of the C ABI.
+struct tgtp_graph {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint64_t n = 0, m = 0;
+    uint32_t max_degree = 0, min_degree = 0;
+    bool has_multi_edges = false;  // a row holds the same neighbour twice (loader keeps them)
+    uint64_t num_forward = 0;      // slots (u, v) with v >= u
+    uint64_t num_active = 0;       // vertices with nonzero degree
+
+    // CSR and derived per-slot maps (device)
+    tgtp::DeviceBuffer idx, adj, deg;
+    tgtp::DeviceBuffer row_of;   // slot -> its row u
+    tgtp::DeviceBuffer rev;      // slot (u,v) -> lower_bound of u in row v
+    tgtp::DeviceBuffer sym_src;  // slot q -> 1 + last slot p with rev[p] == q (0: none)
+    tgtp::DeviceBuffer forward;  // slots with v >= u, in CSR order
+
+    // eigenpairs
+    uint32_t omega = 0;
+    std::vector<double> values;  // host copy (constants of the tau bound are formed on the host)
+    tgtp::DeviceBuffer d_values, vec_f32, vec_f64, vec_bf16;
+    // tau-bound constants: onep[i] = 1 + lambda_i, onem[i] = 1 - lambda_i and the powers
+    // lambda_i^(2(k+1)) for k < kTauTableRows, formed by the reference's repeated multiplication
+    tgtp::DeviceBuffer onep, onem, etab, etab_f;
+    bool has_f32 = false, has_f64 = false, has_bf16 = false;
+
+    // run scratch
+    tgtp::DeviceBuffer taus, preds, stats, counters, sums, work, scratch, out;
+    int32_t last_precision = -1;
+    bool have_run = false;
+
+    tgtp::Profiler prof;
+
+    ~tgtp_graph();
+};
+
+namespace tgtp {
+void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_counters);
+void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* host_sums3);
+void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores);
+void graph_prepare(tgtp_graph* g);
+}  // namespace tgtp
