@@ -1,0 +1,362 @@
+"""Benchmark of the tgtp hot path on B200.
+
+Headline workload (one GPU): tgtp() on a seeded Chung-Lu graph, n = 4,039, 88,234 undirected edges,
+degree exponent 2.5, omega = 128 eigenpairs (scipy restatement of the reference's eigen prep),
+gamma = 10, epsilon = 0.05, in the plain FP64 form.  A step is one tgtp() call over that graph;
+metric: undirected edges scored per second (the reference's benchmark.cpp timing scope).  The same
+line carries the other forms and the SABA walk counter (transitions per second) as extra keys.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`  = device time (CUDA events on the launching stream) of K steps, inputs resident in HBM,
+           L2 flushed (256 MiB write) before every step, outside the events.
+`e2e`    = the same metric through the public API with pinned host buffers: graph + eigen upload,
+           tgtp_run, score download and graph release inside every step.
+`roofline` = the dominant kernel's algorithmic bytes per launch / its event-timed launch time.
+N > 1: one process per GPU (torchrun), every rank scores its own graph (seed + rank): weak scaling,
+no collective on the data path; the slowest rank's time counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "walk transitions/s; AESC edges/s at ε, mixed vs FP64 on 1 B200; % HBM peak"
+N_VERT, N_EDGES, EXPONENT, OMEGA, GAMMA, EPS = 4039, 88234, 2.5, 128, 10, 0.05
+WORKLOAD = ("tgtp AESC, plain FP64 form: Chung-Lu n=4039 E=88234 exp 2.5 (LCC), omega=128, "
+            "gamma=10, eps=0.05")
+L2_FLUSH_BYTES = 256 << 20
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_inputs(seed: int, folder: str):
+    """graph.txt + sorted_eigens_128.txt for the headline graph (cached by seed)."""
+    from tgtp_b200 import eigenprep, synth
+
+    g = synth.chung_lu(N_VERT, N_EDGES, EXPONENT, seed)
+    os.makedirs(folder, exist_ok=True)
+    gpath = os.path.join(folder, "graph.txt")
+    epath = os.path.join(folder, f"sorted_eigens_{OMEGA}.txt")
+    if not os.path.exists(epath):
+        synth.write_graph_txt(g, gpath)
+        eigenprep.eigenprep_folder(folder, OMEGA)
+    return g, gpath, epath
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int, warmups: int):
+    """The reference's own benchmark binary (compiled from its sources into oracle/_ref)."""
+    import oracle
+
+    exe = oracle.ref_binary("benchmark")
+    if exe is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([exe, dataset, str(EPS), str(threads), str(repeats), folder_root,
+                        str(OMEGA), str(GAMMA), str(warmups)], capture_output=True, text=True,
+                       env=env, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError("reference benchmark failed: " + r.stderr[-400:])
+    secs = [float(line.split("\t")[5]) for line in r.stdout.splitlines()[1:] if line.strip()]
+    return secs
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    root = tempfile.mkdtemp(prefix="tgtp_bench_ref_")
+    g, _, _ = make_inputs(1, os.path.join(root, "cl4039"))
+    threads = os.cpu_count() or 1
+    secs = cpu_reference_run(root, "cl4039", threads, args.steps, args.warmup)
+    if secs is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference binaries were not built (oracle/_ref missing)"}))
+        return 0
+    mean = statistics.mean(secs)
+    value = g.num_edges / mean
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Chung-Lu + scipy eigenpairs)",
+        "config": {"workload": WORKLOAD, "graph_seed": 1, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} timed tgtp() calls after {args.warmup} warm-up, "
+                                   "reference benchmark binary (-Ofast -march=x86-64-v3, OpenMP)"},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_FP32, PRECISION_FP64,
+                                VEC_F32, VEC_F64, load_eigens_txt, saba_count)
+
+    seed = 1 + rank
+    root = tempfile.mkdtemp(prefix=f"tgtp_bench_r{rank}_")
+    g, gpath, epath = make_inputs(seed, os.path.join(root, "cl4039"))
+    idx, adj = g.csr()
+    n, m, E = g.n, int(idx[-1]), g.num_edges
+    values, v32, v64 = load_eigens_txt(epath, n, OMEGA)
+
+    stream = torch.cuda.current_stream()
+    dg = AESCGraph.from_csr(idx, adj)
+    dg.set_stream(stream.cuda_stream)
+    dg.upload_eigens(values, v64, VEC_F64)
+    dg.upload_eigens(values, v32, VEC_F32)
+    out = torch.empty(m, dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def timed(form: int, steps: int, warmup: int, profile: bool):
+        a = AESC(dg, AESCConfig(EPS, omega=OMEGA, gamma=GAMMA, precision=form))
+        for _ in range(warmup):
+            a.tgtp_device(out.data_ptr())
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        barrier()
+        torch.cuda.synchronize()
+        dg.set_profiling(profile)
+        t0 = time.perf_counter()
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            a.tgtp_device(out.data_ptr())
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        barrier()
+        kstats = dg.kernel_stats() if profile else {}
+        dg.set_profiling(False)
+        ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+        return ms, wall, kstats, a.stats()
+
+    # ---- headline: FP64 form, inputs resident ----
+    with ClockSampler(local) as clocks:
+        ms64, wall64, k64, st64 = timed(PRECISION_FP64, args.steps, args.warmup, True)
+    out64 = out.clone()
+    ms32, _, k32, st32 = timed(PRECISION_FP32, max(args.steps // 4, 10), args.warmup, True)
+
+    dev_ms = torch.tensor([ms64 / args.steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(dev_ms, op=torch.distributed.ReduceOp.MAX)
+    ms_step = float(dev_ms.item())
+    value = world * E / (ms_step * 1e-3)
+
+    # ---- e2e: public API with pinned host buffers ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_idx, h_adj, h_vals, h_vec = pin(idx), pin(adj), pin(values), pin(v64)
+    h_out = torch.empty(m, dtype=torch.float32).pin_memory()
+    h2d = h_idx.numel() * 4 + h_adj.numel() * 4 + h_vals.numel() * 8 + h_vec.numel() * 8
+    d2h = m * 4
+
+    def e2e_step():
+        eg = AESCGraph.from_csr(h_idx.numpy(), h_adj.numpy())
+        eg.upload_eigens(h_vals.numpy(), h_vec.numpy(), VEC_F64)
+        from tgtp_b200 import _lib
+        import ctypes as C
+
+        cfg = AESCConfig(EPS, omega=OMEGA, gamma=GAMMA, precision=PRECISION_FP64).to_c(n)
+        _lib.check(_lib.lib().tgtp_run(eg.handle, C.byref(cfg), C.c_void_p(h_out.data_ptr())))
+        eg.free()
+
+    for _ in range(3):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * E / float(e2e_t.item())
+    # parity guard on the e2e output (same scores as the resident run)
+    ok_e2e = bool(np.array_equal(h_out.numpy(), out64.cpu().numpy()))
+
+    line = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        # dominant kernel of the FP64 form and its algorithmic bytes (tau: 2 omega 8-byte reads
+        # per undirected edge; source: 20 B per push traversal + 12 B per frontier vertex +
+        # 32 B per 2-walker hop; symmetrise: 12 B per slot)
+        per_launch = {
+            "tau": 2 * OMEGA * 8 * E,
+            "source": 20 * st64["push_traversals"] + 12 * st64["push_vertices"]
+                      + 32 * st64["walk_hops"],
+            "symmetrize": 12 * m,
+        }
+        top = max(k64, key=lambda k: k64[k][1])
+        launches, tot = k64[top]
+        avg_ms = tot / launches
+        achieved = per_launch[top] / (avg_ms * 1e-3) / 1e9
+        share = {k: round(v[1] / sum(x[1] for x in k64.values()), 4) for k, v in k64.items()}
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get(f"fp64_{top}")
+            except Exception:
+                traffic = None
+
+        # ---- SABA walk counter on the same graph (the reference's rw_experiment_saba) ----
+        for _ in range(3):
+            saba_count(dg, 5, 2048, counters=False)
+        dg.set_profiling(True)
+        for _ in range(10):
+            saba_count(dg, 5, 2048, counters=False)
+        ks = dg.kernel_stats()
+        dg.set_profiling(False)
+        saba_ms = ks["saba_walk"][1] / ks["saba_walk"][0]
+        trans = n * 2048 * 5
+        saba = {"workload": "SABA d5 w2048 on the same graph", "transitions_per_s":
+                trans / (saba_ms * 1e-3), "kernel_ms": saba_ms,
+                "hbm_frac_of_" + peak_kind: trans * 20 / (saba_ms * 1e-3) / 1e9 / hbm}
+
+        cpu = None
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            secs = cpu_reference_run(root, "cl4039", threads, 5, 1)
+            if secs:
+                cpu = {"value": E / min(secs), "unit": "edges/s", "cores": threads,
+                       "kind": "reference",
+                       "sample": "min of 5 tgtp() calls (after 1 warm-up) of the reference "
+                                 "benchmark binary on the same graph and eigen files"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Chung-Lu graph + scipy eigenpairs)",
+            "config": {"workload": WORKLOAD, "graph_seed": "1 + rank",
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": per_launch[top]},
+            "kernel_share": share,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "matches_resident_run": ok_e2e},
+            "gpu_launches": int(sum(v[0] for v in k64.values())),
+            "clocks": clocks.summary(),
+            "forms": {"fp64": {"edges_per_s": value / world, "ms_per_step": ms_step},
+                      "fp32_reference_arithmetic": {"edges_per_s": E / (ms32 / max(args.steps // 4, 10) * 1e-3),
+                                                    "kernel_ms": {k: v[1] / v[0] for k, v in k32.items()}}},
+            "saba": saba,
+            "wall_s_timed_region": wall64,
+        }
+        print(json.dumps(line))
+    dg.free()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
