@@ -12,6 +12,9 @@
 // one counter with a fire-and-forget atomic that is off that chain.  Counters of vertex ids below
 // `hot` live in shared memory per block (hubs have low ids in the power-law generators, and every
 // id is hot when n is small) and are flushed once at the end; the rest go to L2 atomics.
+#include <algorithm>
+#include <mutex>
+
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -168,3 +171,119 @@ void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* ho
 }
 
 }  // namespace tgtp
+
+// ---- walk counter that allocates nothing -------------------------------------------------------
+//
+// Some callers cannot allocate device memory when they want the walk summary: a process whose
+// device memory is owned by another allocator (a framework arena or a fixed budget that a stray
+// cudaMalloc would overrun), or a latency-critical loop where cudaMalloc/cudaFree would synchronise
+// the whole device.  saba_count_static serves them: the caller passes the CSR already on the device
+// and receives the summary the walk runner prints; the per-vertex counters and the three sums live
+// in the fixed array below, which every GPU that loads this library holds until the process exits.
+namespace tgtp {
+namespace {
+
+// Largest vertex count saba_count_static accepts (16 MiB of uint32 counters).
+constexpr uint64_t kStaticSabaMaxVertices = uint64_t(1) << 22;
+// Words 0..7: four uint64 sums (visit count, checksum, fallback bouquets, active vertices);
+// counters start at word 64 (byte 256).
+constexpr uint64_t kStaticSabaHeaderWords = 64;
+
+__device__ __align__(256) uint32_t g_static_saba_scratch[kStaticSabaHeaderWords + kStaticSabaMaxVertices];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kMaxDevices] = {};
+int g_static_sms[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per device.
+void* static_scratch(int device, int* num_sms) {
+    if (device < 0 || device >= kMaxDevices) fail(TGTP_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[device]) {
+        void* p = nullptr;
+        TGTP_CUDA(cudaGetSymbolAddress(&p, g_static_saba_scratch));
+        int sms = 0;
+        TGTP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        g_static_sms[device] = sms;
+        g_static_addr[device] = p;
+    }
+    *num_sms = g_static_sms[device];
+    return g_static_addr[device];
+}
+
+__global__ void static_active_kernel(const uint32_t* __restrict__ idx, uint64_t n,
+                                     unsigned long long* __restrict__ active) {
+    unsigned long long a = 0;
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+         v += uint64_t(gridDim.x) * blockDim.x)
+        a += idx[v + 1] != idx[v];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(kFullMask, a, o);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(active, a);
+}
+
+}  // namespace
+}  // namespace tgtp
+
+extern "C" tgtp_status saba_count_static(const uint32_t* device_idx, const uint32_t* device_adj,
+                                         uint64_t n, uint32_t depth, uint32_t n_walks,
+                                         void* cuda_stream, saba_result* out) {
+    using namespace tgtp;
+    return guarded([&] {
+        if (!device_idx || !device_adj || !out) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
+        if (n == 0) fail(TGTP_ERR_INVALID_ARGUMENT, "empty graph");
+        if (n > kStaticSabaMaxVertices)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "saba_count_static accepts at most 4194304 vertices (its counters are a fixed "
+                 "16 MiB device array); use saba_count for larger graphs");
+        if (n_walks % 8 != 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "n_walks must be a multiple of 8 within the 32-bit grid domain");
+        int device = 0;
+        TGTP_CUDA(cudaGetDevice(&device));
+        int num_sms = 0;
+        auto* base = static_cast<uint32_t*>(static_scratch(device, &num_sms));
+        auto* sums = reinterpret_cast<unsigned long long*>(base);
+        uint32_t* counters = base + kStaticSabaHeaderWords;
+        cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+        // the array keeps the previous call's contents: start from zero
+        TGTP_CUDA(cudaMemsetAsync(base, 0, sizeof(uint32_t) * (kStaticSabaHeaderWords + n), s));
+        static_active_kernel<<<unsigned(std::min<uint64_t>((n + 255) / 256, 4u * num_sms)), 256, 0, s>>>(
+            device_idx, n, sums + 3);
+        TGTP_LAUNCH_CHECK("static_active_kernel");
+        if (n_walks && depth) {
+            const uint32_t bouquets_per_src = n_walks / 8;
+            const uint32_t grid_step = UINT32_MAX / n_walks;
+            const uint64_t total = n * uint64_t(bouquets_per_src);
+            const uint32_t hot = uint32_t(n < kSabaHotCap ? n : kSabaHotCap);
+            const size_t smem = sizeof(uint32_t) * hot;
+            TGTP_CUDA(cudaFuncSetAttribute(saba_walk_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(sizeof(uint32_t) * kSabaHotCap)));
+            int per_sm = 0;
+            TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, saba_walk_kernel,
+                                                                    kSabaThreads, smem));
+            if (per_sm < 1) per_sm = 1;
+            uint64_t blocks = uint64_t(num_sms) * per_sm;
+            const uint64_t need = (total + 3) / 4 / (kSabaThreads / 32) + 1;
+            if (blocks > need) blocks = need;
+            saba_walk_kernel<<<unsigned(blocks), kSabaThreads, smem, s>>>(
+                device_idx, device_adj, depth, bouquets_per_src, grid_step, total, counters, hot,
+                sums + 2);
+            TGTP_LAUNCH_CHECK("saba_walk_kernel");
+        }
+        const unsigned blocks = unsigned(std::min<uint64_t>((n + 255) / 256, 4u * num_sms));
+        saba_sums_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(counters, n, sums);
+        TGTP_LAUNCH_CHECK("saba_sums_kernel");
+        unsigned long long h[4];
+        TGTP_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s));
+        TGTP_CUDA(cudaStreamSynchronize(s));
+        out->visit_count = h[0];
+        out->checksum = h[1];
+        out->fallback_bouquets = h[2];
+        const unsigned __int128 expect = (unsigned __int128)h[3] * n_walks * depth;
+        if ((unsigned __int128)h[0] != expect)
+            fail(TGTP_ERR_OVERFLOW, "a uint32 visit counter overflowed");
+    });
+}
