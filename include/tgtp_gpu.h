@@ -82,6 +82,9 @@ typedef struct {
     uint64_t tau_iterations;    /* delta-term evaluations of the tau bound               */
     uint64_t tau_ambiguous;     /* tau bounds whose ceil() argument lay within 1e-12 of an
                                    integer (where a last-place libm difference could matter)  */
+    uint64_t phase_cycles[8];   /* SM cycles of the per-source kernel by phase, summed over
+                                   warps: claim/init, push, post-push, cost test, edge bound,
+                                   chi/walk counts, walks, reset                               */
 } tgtp_run_stats;
 
 typedef struct {

@@ -36,10 +36,15 @@ class Config(C.Structure):
 class RunStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in (
         "push_rounds", "push_vertices", "push_traversals", "walk_edges", "walk_count",
-        "walk_hops", "fallback_bouquets", "tau_iterations", "tau_ambiguous")]
+        "walk_hops", "fallback_bouquets", "tau_iterations", "tau_ambiguous")] + [
+        ("phase_cycles", C.c_uint64 * 8)]
+
+    PHASES = ("init", "push", "post_push", "cost_test", "edge_bound", "chi_nr", "walks", "reset")
 
     def as_dict(self):
-        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "phase_cycles"}
+        d["phase_cycles"] = dict(zip(self.PHASES, (int(x) for x in self.phase_cycles)))
+        return d
 
 
 class SabaResult(C.Structure):

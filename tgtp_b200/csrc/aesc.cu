@@ -24,6 +24,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <string>
 #include <type_traits>
 
 #include "common.cuh"
@@ -32,10 +33,13 @@
 namespace tgtp {
 namespace {
 
-constexpr int kTauThreads = 128;
-constexpr int kSrcWarps = 4;
-constexpr int kSrcThreads = kSrcWarps * 32;
+constexpr int kTauThreads = 32;
+constexpr int kSrcMaxThreads = 128;
+constexpr int kPushAhead = 4;         // adjacency chunks loaded ahead in the push
+constexpr int kB = 4;                 // 32-wide chunks per pipelined load step
 constexpr int kTopK = 16;            // register top-k used for gamma <= 16
+// per-warp shared scratch of the chi step: 64 u64 max/min images + 33 + 32 u32 slot offsets
+constexpr size_t kAccBytes = 1024;
 constexpr int kTauTableRows = 64;    // rows of the eigen_t_1 power table (api.cu)
 constexpr uint64_t kMaxWalks = 0xffffffffull;  // nr beyond the 32-bit grid is not supported
 
@@ -43,7 +47,8 @@ enum : unsigned { kErrDeadline = 1u, kErrWalkCount = 2u };
 
 enum StatIdx {
     kStPushRounds = 0, kStPushVertices, kStPushTraversals, kStWalkEdges, kStWalkCount,
-    kStWalkHops, kStFallback, kStTauIters, kStTauAmbiguous, kStCount
+    kStWalkHops, kStFallback, kStTauIters, kStTauAmbiguous, kStPhase0,
+    kStCount = kStPhase0 + 8
 };
 
 struct TauConst {
@@ -91,63 +96,179 @@ __device__ __forceinline__ Real etab_value(const Real* tab, const double* tabd, 
 }
 
 // ---- stage 1: tau per undirected edge ------------------------------------------------------------
+// A warp takes 32 forward slots (one lane each) and sweeps the eigen index i in chunks of 32.  For
+// each chunk the 32 edges' x_u and x_v pieces are copied into shared memory with asynchronous
+// copies (every copy of the chunk in flight at once, coalesced 128/256-byte rows), double buffered
+// so the next chunk streams in while the lanes consume the current one from odd-stride tiles
+// (conflict-free).  Each lane keeps its edge's sums in index order, exactly as the reference does:
+// the first sweep carries upsilon and the first delta term together (two independent chains), any
+// further delta iteration takes one more sweep.
+__device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* gsrc, int bytes) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// x / y for a positive divisor known in advance, correctly rounded (round to nearest even), with
+// Markstein's method (P. Markstein, IBM J. Res. Dev. 34(1), 1990): q0 = x * r with r = RN(1/y) and
+// one correction q1 = q0 + r * (x - q0 y), remainders exact by FMA.  The result is then checked:
+// with rho = x - q1 y exact, q1 = RN(x / y) when |rho| < y * (half the gap from q1 to its
+// neighbour on x / y's side): half an ulp of q1, a quarter ulp below a power of two.  Whenever the
+// check cannot prove it (x zero or negative, q1 out of the safe exponent range, a divisor the host
+// marked with r = NaN), the quotient comes from the correctly rounded division instead.
+__device__ __forceinline__ double div_fixed(double x, double y, double r) {
+    const double q0 = __dmul_rn(x, r);
+    const double q1 = __fma_rn(__fma_rn(-q0, y, x), r, q0);
+    const double rho = __fma_rn(-q1, y, x);
+    const unsigned hi = unsigned(__double2hiint(q1));
+    const unsigned e = hi >> 20;  // sign bit clear for positive q1
+    double half = __hiloint2double(int((e - 53u) << 20), 0);
+    if (((hi & 0xfffffu) | unsigned(__double2loint(q1))) == 0u && rho < 0.0) half *= 0.5;
+    const bool ok = (e - 65u) < (0x600u - 65u) && fabs(rho) < __dmul_rn(y, half);
+    return ok ? q1 : __ddiv_rn(x, y);
+}
+
 template <class Real>
 __global__ void __launch_bounds__(kTauThreads)
 tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
            const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ rev,
            const uint32_t* __restrict__ forward, uint64_t num_forward,
            const Real* __restrict__ vec, uint32_t stride, uint32_t omega,
-           const double* __restrict__ onep, const double* __restrict__ onem,
+           const double* __restrict__ onep_g, const double* __restrict__ onem_g,
            const Real* __restrict__ etab, const double* __restrict__ etabd, Real epsilon,
            uint64_t m, TauConst c, int* __restrict__ taus, unsigned long long* __restrict__ stats) {
+    constexpr uint32_t CH = 128 / sizeof(Real);  // chunk: one 128-byte row piece
+    constexpr uint32_t LD = CH + 1;              // odd tile stride: conflict-free own-row reads
+    extern __shared__ __align__(16) unsigned char tsm[];
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t wpb = blockDim.x >> 5;
+    // per index: (1 + lambda_i, 1 - lambda_i) and (RN(1 / (1 - lambda_i)), eigen_t_1 row 0)
+    double2* cA = reinterpret_cast<double2*>(tsm);
+    double2* cB = cA + omega;
+    Real* tiles = reinterpret_cast<Real*>(cB + omega) + size_t(wib) * 4 * 32 * LD;  // [2][U,V][32][LD]
+    for (uint32_t i = threadIdx.x; i < omega; i += blockDim.x) {
+        const double y = onem_g[i];
+        const double r = (y > 1e-150 && y < 8.0) ? __drcp_rn(y) : __longlong_as_double(0x7ff8000000000000ull);
+        cA[i] = make_double2(onep_g[i], y);
+        cB[i] = make_double2(r, double(etab[i]));
+    }
+    __syncthreads();
     unsigned long long iters = 0, ambiguous = 0;
     const Real mreal = from_u64<Real>(m);
-    for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < num_forward;
-         e += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t pos = __ldg(forward + e);
-        const uint32_t u = __ldg(row_of + pos), v = __ldg(adj + pos);
-        const Real* uf = vec + size_t(u) * stride;
-        const Real* vf = vec + size_t(v) * stride;
-        const uint32_t du = __ldg(idx + u + 1) - __ldg(idx + u);
-        const uint32_t dv = __ldg(idx + v + 1) - __ldg(idx + v);
-        // get_upsilon (:151-162)
-        Real ups = 0;
-        for (uint32_t i = 1; i + 1 < omega; ++i) {
-            const Real diff = rsub(__ldg(uf + i), __ldg(vf + i));
-            ups = from_f64<Real>(__dadd_rn(double(ups), __dmul_rn(double(rmul(diff, diff)),
-                                                                  __ldg(onep + i))));
+    const uint64_t nw = uint64_t(gridDim.x) * wpb;
+    const uint32_t nchunks = (omega + CH - 1) / CH;
+    // lanes stage CH consecutive indices of 32 / CH edges per step
+    constexpr uint32_t EPS = 32 / CH;  // edges per staging step (1 for float, 2 for double)
+    const uint32_t sub = lane / CH, col = lane % CH;
+    for (uint64_t base = (uint64_t(blockIdx.x) * wpb + wib) * 32; base < num_forward; base += nw * 32) {
+        const uint64_t e = base + lane;
+        const bool act = e < num_forward;
+        uint32_t pos = 0, u = 0, v = 0, du = 0, dv = 0;
+        if (act) {
+            pos = __ldg(forward + e);
+            u = __ldg(row_of + pos);
+            v = __ldg(adj + pos);
+            du = __ldg(idx + u + 1) - __ldg(idx + u);
+            dv = __ldg(idx + v + 1) - __ldg(idx + v);
         }
-        ups = rdiv(ups, mreal);
-        int tau = get_tau<Real>(du, dv, epsilon, c.one_m_l1sq, c.b1, Real(0), Real(0), ambiguous);
-        int t = 1;
-        for (uint32_t k = 0;; ++k) {
-            // get_delta (:137-150) with eigen_t_1 = lambda^(2(k+1))
-            Real del = 0;
-            for (uint32_t i = 1; i + 1 < omega; ++i) {
-                const Real diff = rsub(__ldg(uf + i), __ldg(vf + i));
-                const Real et = etab_value<Real>(etab, etabd, stride, k, i);
-                del = from_f64<Real>(__dadd_rn(double(del), __ddiv_rn(double(rmul(rmul(diff, diff), et)),
-                                                                      __ldg(onem + i))));
+        const uint32_t cnt = uint32_t(min(uint64_t(32), num_forward - base));
+        auto stage = [&](uint32_t chunk, uint32_t buf) {
+            Real* U = tiles + size_t(buf) * 2 * 32 * LD;
+            Real* V = U + 32 * LD;
+            const uint32_t i = chunk * CH + col;
+            for (uint32_t t0 = 0; t0 < cnt; t0 += EPS) {
+                const uint32_t t = t0 + sub;
+                const uint32_t ut = __shfl_sync(kFullMask, u, t & 31u);
+                const uint32_t vt = __shfl_sync(kFullMask, v, t & 31u);
+                if (t < cnt && i < omega) {
+                    cp_async_elem(U + t * LD + col, vec + size_t(ut) * stride + i, int(sizeof(Real)));
+                    cp_async_elem(V + t * LD + col, vec + size_t(vt) * stride + i, int(sizeof(Real)));
+                }
             }
-            del = rdiv(del, mreal);
-            ++iters;
-            const int tp = get_tau<Real>(du, dv, epsilon, c.one_m_l2sq, c.b2, del, ups, ambiguous);
-            if (t <= tp && tp < tau) {
-                tau = tp;
-                t += 2;
-            } else {
-                break;
+            cp_async_commit();
+        };
+        Real ups = 0, del = 0;
+        int tau = 0, t = 1;
+        bool done = !act;
+        for (uint32_t k = 0; __any_sync(kFullMask, !done); ++k) {
+            del = Real(0);
+            stage(0, 0);
+            for (uint32_t ch = 0; ch < nchunks; ++ch) {
+                if (ch + 1 < nchunks) {
+                    stage(ch + 1, (ch + 1) & 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncwarp();
+                if (!done) {
+                    const Real* U = tiles + size_t(ch & 1) * 2 * 32 * LD + lane * LD;
+                    const Real* V = U + 32 * LD;
+                    const uint32_t i0 = ch * CH;
+                    const uint32_t lo = i0 == 0 ? 1u : 0u;
+                    const uint32_t hi = min(CH, omega - 1 - i0);  // indices i < omega - 1
+                    // get_upsilon (:151-162) with get_delta (:137-150) at eigen_t_1 = lambda^2,
+                    // or get_delta alone at lambda^(2(k+1))
+                    auto term0 = [&](uint32_t j) {
+                        const uint32_t i = i0 + j;
+                        const Real d = rsub(U[j], V[j]);
+                        const Real d2 = rmul(d, d);
+                        const double2 a = cA[i], b = cB[i];
+                        ups = from_f64<Real>(__dadd_rn(double(ups), __dmul_rn(double(d2), a.x)));
+                        del = from_f64<Real>(__dadd_rn(
+                            double(del), div_fixed(double(rmul(d2, Real(b.y))), a.y, b.x)));
+                    };
+                    auto termk = [&](uint32_t j) {
+                        const uint32_t i = i0 + j;
+                        const Real d = rsub(U[j], V[j]);
+                        const Real et = etab_value<Real>(etab, etabd, stride, k, i);
+                        const double2 a = cA[i], b = cB[i];
+                        del = from_f64<Real>(__dadd_rn(
+                            double(del), div_fixed(double(rmul(rmul(d, d), et)), a.y, b.x)));
+                    };
+                    if (k == 0) {
+                        if (lo == 0 && hi == CH) {
+#pragma unroll
+                            for (uint32_t j = 0; j < CH; ++j) term0(j);
+                        } else {
+                            for (uint32_t j = lo; j < hi; ++j) term0(j);
+                        }
+                    } else {
+                        for (uint32_t j = lo; j < hi; ++j) termk(j);
+                    }
+                }
+                __syncwarp();
+            }
+            if (!done) {
+                if (k == 0) {
+                    ups = rdiv(ups, mreal);
+                    tau = get_tau<Real>(du, dv, epsilon, c.one_m_l1sq, c.b1, Real(0), Real(0), ambiguous);
+                }
+                del = rdiv(del, mreal);
+                ++iters;
+                const int tp = get_tau<Real>(du, dv, epsilon, c.one_m_l2sq, c.b2, del, ups, ambiguous);
+                if (t <= tp && tp < tau) {
+                    tau = tp;
+                    t += 2;
+                } else {
+                    done = true;
+                    taus[pos] = tau;
+                    taus[__ldg(rev + pos)] = tau;
+                }
             }
         }
-        taus[pos] = tau;
-        taus[__ldg(rev + pos)] = tau;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         iters += __shfl_xor_sync(kFullMask, iters, o);
         ambiguous += __shfl_xor_sync(kFullMask, ambiguous, o);
     }
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         if (iters) atomicAdd(stats + kStTauIters, iters);
         if (ambiguous) atomicAdd(stats + kStTauAmbiguous, ambiguous);
     }
@@ -171,7 +292,7 @@ struct SourceParams {
     uint32_t* qbuf;       // 2 * n per warp
     WalkItem* items;      // max_degree per warp
     Real* pvec_g;         // n per warp (global tier)
-    uint32_t* vis_g;      // ceil(n/32) per warp (global tier)
+    unsigned char* vis_g; // n per warp (global tier)
     size_t smem_per_warp;
     uint32_t max_degree;
     double eps;
@@ -179,6 +300,7 @@ struct SourceParams {
     int gamma;
     int* ell_out;
     unsigned long long* stats;
+    const uint2* adjd;    // (neighbour, neighbour degree) per slot
     uint64_t budget_ns;   // device time budget; past it every warp stops and flags a timeout
 };
 
@@ -200,9 +322,34 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x)
     return x;
 }
 
-__device__ __forceinline__ bool vis_test_set(uint32_t* vis, uint32_t u) {
-    const uint32_t bit = 1u << (u & 31);
-    return !(atomicOr(vis + (u >> 5), bit) & bit);
+// Runs over [0, count) in steps of 32 * kB: load(i0, regs) issues the loads of one step into
+// registers, proc(i0, regs) consumes them.  The next step's loads are issued before the current
+// step is processed, so a pass over a frontier or a row waits for memory once, not once per step.
+template <class T, class Load, class Proc>
+__device__ __forceinline__ void pipelined(uint32_t count, Load load, Proc proc) {
+    if (count == 0) return;
+    T a[kB], b[kB];
+    load(0u, a);
+    for (uint32_t i0 = 0; i0 < count; i0 += 32 * kB) {
+        if (i0 + 32 * kB < count) load(i0 + 32 * kB, b);
+        proc(i0, a);
+#pragma unroll
+        for (int k = 0; k < kB; ++k) a[k] = b[k];
+    }
+}
+
+// Order-preserving integer images of non-negative reals (residuals are never negative), so that
+// shared-memory integer atomics give max / min.
+__device__ __forceinline__ unsigned long long ord_bits(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ unsigned long long ord_bits(double x) {
+    return (unsigned long long)__double_as_longlong(x);
+}
+template <class Real> __device__ __forceinline__ Real from_ord(unsigned long long b);
+template <> __device__ __forceinline__ float from_ord<float>(unsigned long long b) {
+    return __uint_as_float(unsigned(b));
+}
+template <> __device__ __forceinline__ double from_ord<double>(unsigned long long b) {
+    return __longlong_as_double((long long)b);
 }
 
 // The real_gamma-th largest residual of the frontier (counting multiplicity) and how many of the
@@ -211,28 +358,39 @@ __device__ __forceinline__ bool vis_test_set(uint32_t* vis, uint32_t u) {
 template <class Real>
 __device__ void kth_largest(const uint32_t* q, uint32_t qs, const Real* pvec, int rg, Real& t,
                             int& n_eq_taken) {
-    const int lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31;
+    auto load_q = [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            const uint32_t i = i0 + 32 * b + lane;
+            r[b] = i < qs ? q[i] : 0xffffffffu;
+        }
+    };
     if (rg <= kTopK) {
         Real L[kTopK];
 #pragma unroll
         for (int j = 0; j < kTopK; ++j) L[j] = Real(-INFINITY);
-        for (uint32_t i = lane; i < qs; i += 32) {
-            const Real x = pvec[q[i]];
-            if (x > L[kTopK - 1]) {
+        pipelined<uint32_t>(qs, load_q, [&](uint32_t, const uint32_t* r) {
 #pragma unroll
-                for (int j = kTopK - 1; j > 0; --j) {
-                    const Real prev = L[j - 1];
-                    L[j] = x > prev ? prev : (x > L[j] ? x : L[j]);
+            for (int b = 0; b < kB; ++b) {
+                if (r[b] == 0xffffffffu) continue;
+                const Real x = pvec[r[b]];
+                if (x > L[kTopK - 1]) {
+#pragma unroll
+                    for (int j = kTopK - 1; j > 0; --j) {
+                        const Real prev = L[j - 1];
+                        L[j] = x > prev ? prev : (x > L[j] ? x : L[j]);
+                    }
+                    L[0] = x > L[0] ? x : L[0];
                 }
-                L[0] = x > L[0] ? x : L[0];
             }
-        }
+        });
         Real last = Real(-INFINITY);
         int run = 0;
         for (int r = 0; r < rg; ++r) {
             const Real mx = warp_max(L[0]);
             const unsigned who = __ballot_sync(kFullMask, L[0] == mx);
-            if (lane == __ffs(who) - 1) {
+            if (lane == uint32_t(__ffs(who) - 1)) {
 #pragma unroll
                 for (int j = 0; j < kTopK - 1; ++j) L[j] = L[j + 1];
                 L[kTopK - 1] = Real(-INFINITY);
@@ -249,17 +407,21 @@ __device__ void kth_largest(const uint32_t* q, uint32_t qs, const Real* pvec, in
     while (true) {
         Real best = Real(-INFINITY);
         unsigned cnt = 0;
-        for (uint32_t i = lane; i < qs; i += 32) {
-            const Real x = pvec[q[i]];
-            if (x < thr) {
-                if (x > best) {
-                    best = x;
-                    cnt = 1;
-                } else if (x == best) {
-                    ++cnt;
+        pipelined<uint32_t>(qs, load_q, [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                if (r[b] == 0xffffffffu) continue;
+                const Real x = pvec[r[b]];
+                if (x < thr) {
+                    if (x > best) {
+                        best = x;
+                        cnt = 1;
+                    } else if (x == best) {
+                        ++cnt;
+                    }
                 }
             }
-        }
+        });
         const Real mx = warp_max(best);
         unsigned c = best == mx ? cnt : 0;
 #pragma unroll
@@ -274,36 +436,70 @@ __device__ void kth_largest(const uint32_t* q, uint32_t qs, const Real* pvec, in
     }
 }
 
+// Segmented max / min over lanes whose segment ids are non-decreasing: after the shuffles, the
+// last lane of each segment holds the segment's extremum.
+template <class Real>
+__device__ __forceinline__ void seg_maxmin(uint32_t seg, Real& mx, Real& mn) {
+    const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Real ymx = __shfl_up_sync(kFullMask, mx, o);
+        const Real ymn = __shfl_up_sync(kFullMask, mn, o);
+        const uint32_t ys = __shfl_up_sync(kFullMask, seg, o);
+        if (lane >= uint32_t(o) && ys == seg) {
+            mx = std_max(mx, ymx);
+            mn = std_min(mn, ymn);
+        }
+    }
+}
+
 template <class Real, bool SMEM>
-__global__ void __launch_bounds__(kSrcThreads)
+__global__ void __launch_bounds__(kSrcMaxThreads)
 source_kernel(SourceParams<Real> p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wib = threadIdx.x >> 5;
-    const uint64_t gw = uint64_t(blockIdx.x) * kSrcWarps + wib;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint64_t gw = uint64_t(blockIdx.x) * wpb + wib;
     const uint32_t n = p.n;
-    const uint32_t nwords = (n + 31) / 32;
+    const unsigned lt = (1u << lane) - 1u;
+    constexpr uint32_t NONE = 0xffffffffu;
     Real* pvec;
-    uint32_t* vis;
+    unsigned char* vis;       // per vertex: 1 = discovered this round, 2 = in the top-gamma set
+    unsigned long long* acc;  // 64 per warp: per-slot neighbourhood max (0..31) / min (32..63)
     if (SMEM) {
         unsigned char* base = smem + size_t(wib) * p.smem_per_warp;
         pvec = reinterpret_cast<Real*>(base);
-        vis = reinterpret_cast<uint32_t*>(base + ((size_t(n) * sizeof(Real) + 15) & ~size_t(15)));
+        const size_t pv = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
+        vis = base + pv;
+        acc = reinterpret_cast<unsigned long long*>(base + pv + ((size_t(n) + 15) & ~size_t(15)));
     } else {
         pvec = p.pvec_g + gw * size_t(n);
-        vis = p.vis_g + gw * size_t(nwords);
+        vis = p.vis_g + gw * size_t(n);
+        acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
-    for (uint32_t i = lane; i < n; i += 32) pvec[i] = Real(0);
-    for (uint32_t i = lane; i < nwords; i += 32) vis[i] = 0;
+    for (uint32_t i = lane; i < n; i += 32) {
+        pvec[i] = Real(0);
+        vis[i] = 0;
+    }
     uint32_t* qa = p.qbuf + gw * 2 * size_t(n);
     uint32_t* qb = qa + n;
     WalkItem* items = p.items + gw * size_t(p.max_degree);
     const uint32_t* __restrict__ idx = p.idx;
     const uint32_t* __restrict__ adj = p.adj;
-    const uint32_t* __restrict__ deg = p.deg;
+    const int* __restrict__ taus = p.taus;
     unsigned long long st_rounds = 0, st_pv = 0, st_tr = 0, st_we = 0, st_wc = 0, st_wh = 0,
                        st_fb = 0;
     const uint64_t deadline = globaltimer_ns() + p.budget_ns;
+    // SM cycles spent per phase of a source (claim/init, push, post-push, cost test, edge bound,
+    // chi/nr, walks, reset), summed over the warp's sources
+    long long ph[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long tmark = clock64();
+    auto lap = [&](int i) {
+        const long long now = clock64();
+        ph[i] += now - tmark;
+        tmark = now;
+    };
     __syncwarp();
 
     while (true) {
@@ -321,8 +517,8 @@ source_kernel(SourceParams<Real> p) {
         const uint32_t rb = __ldg(idx + src), re = __ldg(idx + src + 1);
         const uint32_t dsi = re - rb;
         const Real ds = from_u64<Real>(dsi);
-        const Real pinit = from_f64<Real>(__ddiv_rn(1.0, double(ds)));  // preds = 1.0 / ds
-        for (uint32_t pos = rb + lane; pos < re; pos += 32) p.preds[pos] = pinit;
+        // preds = 1.0 / ds (:468-470); stored together with the first round's update below
+        const Real pinit = from_f64<Real>(__ddiv_rn(1.0, double(ds)));
         if (lane == 0) {
             pvec[src] = Real(1);
             q[0] = src;
@@ -331,12 +527,34 @@ source_kernel(SourceParams<Real> p) {
         int ell = 0;
         Real gmin, gmax;
         bool timed_out = false;
+        // row loaders (slot id, neighbour, tau) for the pipelined passes over the source's row
+        auto load_adj = [&](uint32_t c, uint32_t* r) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                const uint32_t o = c + 32 * b + lane;
+                r[b] = o < dsi ? __ldg(adj + rb + o) : NONE;
+            }
+        };
+        auto load_tau = [&](uint32_t c, int* r) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                const uint32_t o = c + 32 * b + lane;
+                r[b] = o < dsi ? __ldg(taus + rb + o) : 0;
+            }
+        };
         __syncwarp();
+        lap(0);
         while (true) {
             // ---- diffuse (:218-239) ----
-            // Frontier vertices are fetched 32 at a time (id and row bounds per lane) and handed
-            // out by shuffle; their order of processing is the frontier order.
+            // The frontier is drained in order, one vertex at a time; the lanes share the
+            // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
+            // touch distinct bytes and words).  Per batch of 32 frontier vertices the adjacency is
+            // cut into 32-slot chunks walked by a cursor; a chunk's (neighbour, degree) pairs are
+            // one coalesced 8-byte load per lane, issued kPushAhead chunks before use.  picost (the
+            // new frontier's degree sum) is summed on discovery.  Every vertex has at least one
+            // chunk: tgtp_run rejects isolated vertices.
             uint32_t qns = 0;
+            unsigned long long pcost = 0;
             st_pv += qs;
             for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
                 uint32_t myv = 0, myb = 0, myd = 0;
@@ -346,104 +564,160 @@ source_kernel(SourceParams<Real> p) {
                     myd = __ldg(idx + myv + 1) - myb;
                 }
                 const uint32_t cnt = min(32u, qs - i0);
-                // first adjacency chunk of the next vertex, loaded one step ahead
-                uint32_t nu = 0, nd = 1;
-                {
-                    const uint32_t vb0 = __shfl_sync(kFullMask, myb, 0);
-                    const uint32_t vd0 = __shfl_sync(kFullMask, myd, 0);
-                    if (lane < vd0) {
-                        nu = __ldg(adj + vb0 + lane);
-                        nd = __ldg(deg + nu);
-                    }
-                }
-                for (uint32_t t = 0; t < cnt; ++t) {
-                    const uint32_t v = __shfl_sync(kFullMask, myv, t);
-                    const uint32_t vb = __shfl_sync(kFullMask, myb, t);
-                    const uint32_t vd = __shfl_sync(kFullMask, myd, t);
-                    const uint32_t cu = nu, cd = nd;
-                    if (t + 1 < cnt) {
-                        const uint32_t vb1 = __shfl_sync(kFullMask, myb, t + 1);
-                        const uint32_t vd1 = __shfl_sync(kFullMask, myd, t + 1);
-                        if (lane < vd1) {
-                            nu = __ldg(adj + vb1 + lane);
-                            nd = __ldg(deg + nu);
-                        }
-                    }
-                    const Real r = pvec[v];
-                    __syncwarp();
-                    if (lane == 0) pvec[v] = Real(0);
-                    __syncwarp();
-                    st_tr += vd;
-                    for (uint32_t c = 0; c < vd; c += 32) {
-                        const uint32_t e = c + lane;
-                        const bool act = e < vd;
-                        uint32_t u = 0, du = 1;
-                        if (act) {
-                            if (c == 0) {
-                                u = cu;
-                                du = cd;
-                            } else {
-                                u = __ldg(adj + vb + e);
-                                du = __ldg(deg + u);
+                uint32_t pt = 0, pc = 0;  // prefetch cursor: batch vertex, chunk offset
+                uint2 cur[kPushAhead];
+                uint32_t ct[kPushAhead], cco[kPushAhead];
+                auto load_group = [&](uint2* dst, uint32_t* dt, uint32_t* dc) {
+#pragma unroll
+                    for (int jj = 0; jj < kPushAhead; ++jj) {
+                        dst[jj] = make_uint2(0u, 1u);
+                        dt[jj] = cnt;
+                        dc[jj] = 0;
+                        if (pt < cnt) {
+                            const uint32_t vb = __shfl_sync(kFullMask, myb, pt);
+                            const uint32_t vd = __shfl_sync(kFullMask, myd, pt);
+                            if (pc + lane < vd) dst[jj] = __ldg(p.adjd + vb + pc + lane);
+                            dt[jj] = pt;
+                            dc[jj] = pc;
+                            pc += 32;
+                            if (pc >= vd) {
+                                ++pt;
+                                pc = 0;
                             }
                         }
-                        const bool fresh = act && vis_test_set(vis, u);
-                        const unsigned bal = __ballot_sync(kFullMask, fresh);
-                        if (fresh) qn[qns + __popc(bal & ((1u << lane) - 1u))] = u;
-                        qns += __popc(bal);
-                        if (act) pvec[u] = radd(pvec[u], rdiv(r, from_u64<Real>(du)));
-                        __syncwarp();
+                    }
+                };
+                load_group(cur, ct, cco);
+                Real r = Real(0);
+                while (ct[0] < cnt) {
+                    uint2 nxt[kPushAhead];
+                    uint32_t nt[kPushAhead], nc[kPushAhead];
+                    load_group(nxt, nt, nc);
+#pragma unroll
+                    for (int jj = 0; jj < kPushAhead; ++jj) {
+                        if (ct[jj] < cnt) {
+                            const uint32_t t = ct[jj], c0 = cco[jj];
+                            const uint32_t vd = __shfl_sync(kFullMask, myd, t);
+                            if (c0 == 0) {
+                                const uint32_t v = __shfl_sync(kFullMask, myv, t);
+                                r = pvec[v];
+                                __syncwarp();
+                                if (lane == 0) pvec[v] = Real(0);
+                                __syncwarp();
+                                st_tr += vd;
+                            }
+                            const bool act = c0 + lane < vd;
+                            const uint32_t cu = cur[jj].x, cd = cur[jj].y;
+                            bool fresh = false;
+                            if (act && vis[cu] == 0) {
+                                vis[cu] = 1;
+                                fresh = true;
+                            }
+                            const unsigned bal = __ballot_sync(kFullMask, fresh);
+                            if (fresh) {
+                                qn[qns + __popc(bal & lt)] = cu;
+                                pcost += cd;
+                            }
+                            qns += __popc(bal);
+                            if (act) pvec[cu] = radd(pvec[cu], rdiv(r, from_u64<Real>(cd)));
+                            __syncwarp();
+                        }
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < kPushAhead; ++jj) {
+                        cur[jj] = nxt[jj];
+                        ct[jj] = nt[jj];
+                        cco[jj] = nc[jj];
                     }
                 }
             }
             __syncwarp();
-            const Real ps = pvec[src];
-            for (uint32_t pos = rb + lane; pos < re; pos += 32)
-                p.preds[pos] = radd(p.preds[pos], rdiv(rsub(ps, pvec[__ldg(adj + pos)]), ds));
-            for (uint32_t i = lane; i < qns; i += 32) vis[qn[i] >> 5] = 0;
+            lap(1);
+            // preds[row] += (pvec[src] - pvec[adj]) / ds (:235-237); the first round adds to the
+            // initial 1 / ds directly
+            {
+                const Real ps = pvec[src];
+                struct SlotPred {
+                    uint32_t w;
+                    Real old;
+                };
+                pipelined<SlotPred>(dsi,
+                    [&](uint32_t c, SlotPred* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t o = c + 32 * b + lane;
+                            r[b].w = NONE;
+                            r[b].old = pinit;
+                            if (o < dsi) {
+                                r[b].w = __ldg(adj + rb + o);
+                                if (ell > 0) r[b].old = p.preds[rb + o];
+                            }
+                        }
+                    },
+                    [&](uint32_t c, const SlotPred* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b)
+                            if (r[b].w != NONE)
+                                p.preds[rb + c + 32 * b + lane] =
+                                    radd(r[b].old, rdiv(rsub(ps, pvec[r[b].w]), ds));
+                    });
+            }
+            // clear the new frontier's flags and take its residual max / min (:484-491; max and
+            // min do not depend on order)
+            Real mx = Real(0), mn = Real(1);
+            pipelined<uint32_t>(qns,
+                [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        const uint32_t i = i0 + 32 * b + lane;
+                        r[b] = i < qns ? qn[i] : NONE;
+                    }
+                },
+                [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        if (r[b] == NONE) continue;
+                        vis[r[b]] = 0;
+                        const Real val = pvec[r[b]];
+                        mx = std_max(mx, val);
+                        mn = std_min(mn, val);
+                    }
+                });
             __syncwarp();
             { uint32_t* tmp = q; q = qn; qn = tmp; }
             qs = qns;
             ++ell;
-            // ---- frontier statistics and the push/walk cost test (:483-502) ----
-            unsigned long long pc = 0;
-            Real mx = Real(0), mn = Real(1);
-            for (uint32_t i = lane; i < qs; i += 32) {
-                const uint32_t v = q[i];
-                pc += __ldg(deg + v);
-                const Real val = pvec[v];
-                mx = std_max(mx, val);
-                mn = std_min(mn, val);
-            }
-            pc = warp_sum_u64(pc);
+            lap(2);
+            // ---- the push/walk cost test (:483-502) ----
+            const double picost = double(warp_sum_u64(pcost));
             gmax = warp_max(mx);
             gmin = warp_min(mn);
             gmin = qs < n ? Real(0) : gmin;
-            const double picost = double(pc);
             const double dse0 = __dmul_rn(double(ds), p.eps);
             const double dse2 = __dmul_rn(dse0, dse0);
             double rw = 0;
-            for (uint32_t c = 0; c < dsi; c += 32) {
-                const uint32_t pos = rb + c + lane;
-                double nrd = 0;
-                bool has = false;
-                if (c + lane < dsi) {
-                    const int rest = __ldg(p.taus + pos) - ell;
-                    if (rest > 0) {
+            pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    const uint32_t o = c + 32 * b + lane;
+                    const int rest = tv[b] - ell;
+                    double nrd = 0;
+                    const bool has = o < dsi && rest > 0;
+                    if (has) {
                         const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
                                                      __dsub_rn(double(gmax), double(gmin)));
                         const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
                         nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
-                        has = true;
+                    }
+                    unsigned hb = __ballot_sync(kFullMask, has);
+                    while (hb) {  // rwcost += nr in slot order
+                        const int l = __ffs(hb) - 1;
+                        hb &= hb - 1;
+                        rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
                     }
                 }
-                unsigned hb = __ballot_sync(kFullMask, has);
-                while (hb) {
-                    const int l = __ffs(hb) - 1;
-                    hb &= hb - 1;
-                    rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
-                }
-            }
+            });
+            lap(3);
             if (picost >= __dmul_rn(25.0, rw)) break;
             if (globaltimer_ns() > deadline) {
                 timed_out = true;
@@ -457,9 +731,26 @@ source_kernel(SourceParams<Real> p) {
         st_rounds += ell;
         if (lane == 0 && p.ell_out) p.ell_out[src] = ell;
 
-        // ---- edge bound (:414-442, :504-506) ----
-        Real edge_max;
-        if (p.gamma == 1) {
+        // slots that still need walks (rest = tau - ell > 0), compacted in slot order
+        uint32_t nitems = 0;
+        pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                const uint32_t o = c + 32 * b + lane;
+                const bool has = o < dsi && tv[b] - ell > 0;
+                const unsigned hb = __ballot_sync(kFullMask, has);
+                if (has)
+                    items[nitems + __popc(hb & lt)] =
+                        WalkItem{rb + o, __ldg(adj + rb + o), uint32_t(tv[b] - ell), 0u, 0ull};
+                nitems += __popc(hb);
+            }
+        });
+        __syncwarp();
+
+        // ---- edge bound (:414-442, :504-506); it only feeds chi of walking slots ----
+        Real edge_max = Real(0);
+        if (nitems == 0) {
+        } else if (p.gamma == 1) {
             edge_max = rmul(Real(2), gmax);
         } else {
             const int nnz = int(qs);
@@ -472,23 +763,28 @@ source_kernel(SourceParams<Real> p) {
                 int need_eq;
                 kth_largest<Real>(q, qs, pvec, rg, t, need_eq);
                 int taken_eq = 0;
-                for (uint32_t i0 = 0; i0 < qs && sc < rg; i0 += 32) {
-                    const uint32_t i = i0 + lane;
-                    uint32_t u = 0;
-                    Real x = Real(-INFINITY);
-                    if (i < qs) {
-                        u = q[i];
-                        x = pvec[u];
-                    }
-                    const bool gt = x > t, eq = x == t;
-                    const unsigned be = __ballot_sync(kFullMask, eq);
-                    const bool take_eq = eq && taken_eq + __popc(be & ((1u << lane) - 1u)) < need_eq;
-                    const bool take = gt || take_eq;
-                    const unsigned bt = __ballot_sync(kFullMask, take);
-                    if (take) set[sc + __popc(bt & ((1u << lane) - 1u))] = u;
-                    sc += __popc(bt);
-                    taken_eq += __popc(__ballot_sync(kFullMask, take_eq));
-                }
+                pipelined<uint32_t>(qs,
+                    [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            r[b] = i < qs ? q[i] : NONE;
+                        }
+                    },
+                    [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const Real x = r[b] != NONE ? pvec[r[b]] : Real(-INFINITY);
+                            const bool gt = x > t, eq = x == t;
+                            const unsigned be = __ballot_sync(kFullMask, eq);
+                            const bool take_eq = eq && taken_eq + __popc(be & lt) < need_eq;
+                            const bool take = (gt || take_eq) && sc < rg;
+                            const unsigned bt = __ballot_sync(kFullMask, take);
+                            if (take) set[sc + __popc(bt & lt)] = r[b];
+                            sc += __popc(bt);
+                            taken_eq += __popc(__ballot_sync(kFullMask, take_eq));
+                        }
+                    });
                 gamma_max = std_min(Real(1), t);
             } else {
                 for (uint32_t i = lane; i < qs; i += 32) set[i] = q[i];
@@ -497,81 +793,174 @@ source_kernel(SourceParams<Real> p) {
             }
             __syncwarp();
             edge_max = radd(gmax, gamma_max);
-            for (int i = lane; i < sc; i += 32) vis_test_set(vis, set[i]);
+            for (int i = lane; i < sc; i += 32) vis[set[i]] = 2;
             __syncwarp();
+            // pairs (u, w) with both in the set and w adjacent to u: the members' adjacency lists
+            // are flattened 32 members at a time so a warp scans them in parallel
             Real best = edge_max;
-            for (int s = 0; s < sc; ++s) {
-                const uint32_t u = set[s];
-                const Real pu = pvec[u];
-                const uint32_t ub = __ldg(idx + u), ue = __ldg(idx + u + 1);
-                for (uint32_t e = ub + lane; e < ue; e += 32) {
-                    const uint32_t w = __ldg(adj + e);
-                    if (vis[w >> 5] & (1u << (w & 31))) best = std_max(best, radd(pu, pvec[w]));
+            for (int s0 = 0; s0 < sc; s0 += 32) {
+                uint32_t ub = 0, ud = 0;
+                Real pu = Real(0);
+                if (s0 + int(lane) < sc) {
+                    const uint32_t u = set[s0 + lane];
+                    pu = pvec[u];
+                    ub = __ldg(idx + u);
+                    ud = __ldg(idx + u + 1) - ub;
+                }
+                uint32_t incl = ud;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                    if (lane >= uint32_t(o)) incl += y;
+                }
+                const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                const uint32_t excl = incl - ud;
+                for (uint32_t e0 = 0; e0 < total; e0 += 32) {
+                    const uint32_t e = e0 + lane;
+                    uint32_t mm = 0;
+#pragma unroll
+                    for (uint32_t step = 16; step; step >>= 1) {
+                        const uint32_t cand = mm + step;
+                        const uint32_t ex = __shfl_sync(kFullMask, excl, cand & 31u);
+                        if (cand < 32u && ex <= e) mm = cand;
+                    }
+                    const uint32_t mb = __shfl_sync(kFullMask, ub, mm);
+                    const uint32_t mex = __shfl_sync(kFullMask, excl, mm);
+                    const Real mpu = __shfl_sync(kFullMask, pu, mm);
+                    if (e < total) {
+                        const uint32_t w = __ldg(adj + mb + (e - mex));
+                        if (vis[w] == 2) best = std_max(best, radd(mpu, pvec[w]));
+                    }
                 }
             }
             edge_max = warp_max(best);
             __syncwarp();
-            for (int i = lane; i < sc; i += 32) vis[set[i] >> 5] = 0;
+            for (int i = lane; i < sc; i += 32) vis[set[i]] = 0;
             __syncwarp();
         }
+        lap(4);
 
-        // ---- chi and walk counts per edge (:508-521) ----
-        Real smax = Real(0), smin = Real(FLT_MAX);
-        for (uint32_t pos = rb + lane; pos < re; pos += 32) {
-            const Real x = pvec[__ldg(adj + pos)];
-            smax = std_max(smax, x);
-            smin = std_min(smin, x);
-        }
-        smax = warp_max(smax);
-        smin = warp_min(smin);
-        uint32_t nitems = 0;
-        for (uint32_t c = 0; c < dsi; c += 32) {
-            const bool has = c + lane < dsi && __ldg(p.taus + rb + c + lane) - ell > 0;
-            unsigned hb = __ballot_sync(kFullMask, has);
-            while (hb) {
-                const int l = __ffs(hb) - 1;
-                hb &= hb - 1;
-                const uint32_t pos = rb + c + l;
-                const uint32_t v = __ldg(adj + pos);
-                const int L = __ldg(p.taus + pos) - ell;
-                Real tmax = Real(0), tmin = Real(FLT_MAX);
-                const uint32_t vb = __ldg(idx + v), ve = __ldg(idx + v + 1);
-                for (uint32_t e = vb + lane; e < ve; e += 32) {
-                    const Real x = pvec[__ldg(adj + e)];
-                    tmax = std_max(tmax, x);
-                    tmin = std_min(tmin, x);
+        // ---- chi and walk counts per edge (:392-412, :508-521) ----
+        // Neighbourhood max / min of the walking slots' targets, 32 slots at a time: their
+        // adjacency lists are concatenated and each lane walks entries lane, lane + 32, ... with a
+        // cursor over the slots' start offsets (in shared memory; entries of a slot are
+        // consecutive, so the cursor rarely moves), keeps its running max / min in registers and
+        // flushes them with one shared atomic when it leaves a slot.  Then each lane forms its
+        // slot's chi and nr with the reference's roundings.
+        if (nitems) {
+            Real smax = Real(0), smin = Real(FLT_MAX);
+            pipelined<uint32_t>(dsi, load_adj, [&](uint32_t, const uint32_t* w) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    if (w[b] == NONE) continue;
+                    const Real x = pvec[w[b]];
+                    smax = std_max(smax, x);
+                    smin = std_min(smin, x);
                 }
-                tmax = warp_max(tmax);
-                tmin = warp_min(tmin);
-                // get_chi (:410): float terms rounded as in the reference, summed in double
-                const double A = __dadd_rn(double(gmax), __ddiv_rn(double(radd(smax, tmax)), 2.0));
-                const double B = __dadd_rn(A, double(rmul(Real(L - 1), edge_max)));
-                const double C = __dsub_rn(__dsub_rn(B, double(smin)), double(tmin));
-                const double E = __dsub_rn(C, double(rmul(Real(2 * (L - 1)), gmin)));
-                const Real chi = from_f64<Real>(E);
-                // nr (:519-521)
-                const Real c8 = rmul(Real(8), rmul(chi, chi));
-                const double num = __dmul_rn(double(c8), p.logmd);
-                const Real dse = from_f64<Real>(__dmul_rn(double(ds), p.eps));
-                const double den = double(rmul(dse, dse));
-                const double nrd = std_max(ceil(__ddiv_rn(num, den)), 1.0);
-                unsigned long long nr = (unsigned long long)nrd;
-                nr += 8ull - (nr % 8ull);
-                if (nr > kMaxWalks) {
-                    if (lane == 0) atomicOr(p.work + 1, kErrWalkCount);
-                    continue;
+            });
+            smax = warp_max(smax);
+            smin = warp_min(smin);
+            const Real dse = from_f64<Real>(__dmul_rn(double(ds), p.eps));
+            const double den = double(rmul(dse, dse));
+            uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64);  // 33 slot offsets
+            uint32_t* vbs = exs + 33;                               // 32 row starts
+            for (uint32_t s0 = 0; s0 < nitems; s0 += 32) {
+                const uint32_t my = s0 + lane;
+                uint32_t vb = 0, vd = 0, L = 0;
+                if (my < nitems) {
+                    const WalkItem it = items[my];
+                    vb = __ldg(idx + it.v);
+                    vd = __ldg(idx + it.v + 1) - vb;
+                    L = it.len;
                 }
-                if (lane == 0) items[nitems] = WalkItem{pos, v, uint32_t(L), 0u, nr};
-                ++nitems;
-                st_we += 1;
-                st_wc += nr;
-                st_wh += nr * (unsigned long long)L;
+                acc[lane] = ord_bits(Real(0));
+                acc[32 + lane] = ord_bits(Real(FLT_MAX));
+                uint32_t incl = vd;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                    if (lane >= uint32_t(o)) incl += y;
+                }
+                const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                exs[lane] = incl - vd;
+                vbs[lane] = vb;
+                if (lane == 31) exs[32] = total;
+                __syncwarp();
+                uint32_t cm = 0;                  // address cursor
+                uint32_t cseg = 32;               // accumulation cursor (32: none yet)
+                Real amx = Real(0), amn = Real(FLT_MAX);
+                auto flush = [&]() {
+                    if (cseg < 32u) {
+                        atomicMax(acc + cseg, ord_bits(amx));
+                        atomicMin(acc + 32 + cseg, ord_bits(amn));
+                    }
+                };
+                struct Ent {
+                    uint32_t seg, w;
+                };
+                pipelined<Ent>(total,
+                    [&](uint32_t e0, Ent* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t e = e0 + 32 * b + lane;
+                            r[b].seg = 32u;
+                            r[b].w = 0u;
+                            if (e < total) {
+                                while (exs[cm + 1] <= e) ++cm;
+                                r[b].seg = cm;
+                                r[b].w = __ldg(adj + vbs[cm] + (e - exs[cm]));
+                            }
+                        }
+                    },
+                    [&](uint32_t, const Ent* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            if (r[b].seg == 32u) continue;
+                            if (r[b].seg != cseg) {
+                                flush();
+                                cseg = r[b].seg;
+                                amx = Real(0);
+                                amn = Real(FLT_MAX);
+                            }
+                            const Real x = pvec[r[b].w];
+                            amx = std_max(amx, x);
+                            amn = std_min(amn, x);
+                        }
+                    });
+                flush();
+                if (my < nitems) {
+                    const Real tmax = from_ord<Real>(acc[lane]);
+                    const Real tmin = from_ord<Real>(acc[32 + lane]);
+                    // get_chi (:410): float terms rounded as in the reference, summed in double
+                    const int Li = int(L);
+                    const double A = __dadd_rn(double(gmax), __ddiv_rn(double(radd(smax, tmax)), 2.0));
+                    const double B = __dadd_rn(A, double(rmul(Real(Li - 1), edge_max)));
+                    const double C = __dsub_rn(__dsub_rn(B, double(smin)), double(tmin));
+                    const double E = __dsub_rn(C, double(rmul(Real(2 * (Li - 1)), gmin)));
+                    const Real chi = from_f64<Real>(E);
+                    // nr (:519-521)
+                    const Real c8 = rmul(Real(8), rmul(chi, chi));
+                    const double num = __dmul_rn(double(c8), p.logmd);
+                    const double nrd = std_max(ceil(__ddiv_rn(num, den)), 1.0);
+                    unsigned long long nr = (unsigned long long)nrd;
+                    nr += 8ull - (nr % 8ull);
+                    if (nr > kMaxWalks) {
+                        atomicOr(p.work + 1, kErrWalkCount);
+                        nr = 0;  // skipped by the walk loop
+                    } else {
+                        st_we += 1;
+                        st_wc += nr;
+                        st_wh += nr * (unsigned long long)L;
+                    }
+                    items[my].nr = nr;
+                }
+                __syncwarp();
             }
         }
-        __syncwarp();
+        lap(5);
 
         // ---- 2-way bouquet walks (:241-391): four bouquets per warp, one per 8-lane group ----
-        {
+        if (nitems) {
             const uint32_t j = lane & 7, grp = lane >> 3;
             uint32_t next = 0;
             bool has = false, start = false, primary = true;
@@ -586,15 +975,17 @@ source_kernel(SourceParams<Real> p) {
                     const uint32_t my = next + rank;
                     if (my < nitems) {
                         it = items[my];
-                        has = true;
-                        start = true;
-                        bi = 0;
-                        x = Real(0);
-                        step = uint32_t(0xffffffffull / it.nr);
+                        if (it.nr) {
+                            has = true;
+                            start = true;
+                            bi = 0;
+                            x = Real(0);
+                            step = uint32_t(0xffffffffull / it.nr);
+                        }
                     }
                 }
                 next += __popc(need);
-                if (!__any_sync(kFullMask, has)) break;
+                if (!__any_sync(kFullMask, has) && next >= nitems) break;
                 if (has && start) {
                     cur = src;
                     cur2 = it.v;
@@ -646,22 +1037,43 @@ source_kernel(SourceParams<Real> p) {
                 }
             }
         }
+        lap(6);
         // ---- next source starts from an all-zero residual vector ----
         __syncwarp();
-        for (uint32_t i = lane; i < qs; i += 32) pvec[q[i]] = Real(0);
+        pipelined<uint32_t>(qs,
+            [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    const uint32_t i = i0 + 32 * b + lane;
+                    r[b] = i < qs ? q[i] : NONE;
+                }
+            },
+            [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b)
+                    if (r[b] != NONE) pvec[r[b]] = Real(0);
+            });
         if (lane == 0) pvec[src] = Real(0);
         __syncwarp();
+        lap(7);
     }
     if (lane == 0) {
         atomicAdd(p.stats + kStPushRounds, st_rounds);
         atomicAdd(p.stats + kStPushVertices, st_pv);
         atomicAdd(p.stats + kStPushTraversals, st_tr);
+    }
+    st_we = warp_sum_u64(st_we);
+    st_wc = warp_sum_u64(st_wc);
+    st_wh = warp_sum_u64(st_wh);
+    st_fb = warp_sum_u64(st_fb);
+    if (lane == 0) {
         atomicAdd(p.stats + kStWalkEdges, st_we);
         atomicAdd(p.stats + kStWalkCount, st_wc);
         atomicAdd(p.stats + kStWalkHops, st_wh);
+        atomicAdd(p.stats + kStFallback, st_fb);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(p.stats + kStPhase0 + i, (unsigned long long)ph[i]);
     }
-    st_fb = warp_sum_u64(st_fb);
-    if (lane == 0) atomicAdd(p.stats + kStFallback, st_fb);
 }
 
 // ---- stage 3: symmetrise -------------------------------------------------------------------------
@@ -720,8 +1132,23 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     TGTP_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned) * 4, s));
 
     {
+        // per block: two double2 constants per index; per warp: two buffers of (x_u, x_v) chunks
+        // of 32 edges x one 128-byte row piece, rows padded by one element
+        const size_t tau_smem = 2 * sizeof(double2) * omega +
+                                size_t(kTauThreads / 32) * 4 * 32 * (128 / sizeof(Real) + 1) * sizeof(Real);
+        if (tau_smem > size_t(227) * 1024)
+            fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel tile");
+        TGTP_CUDA(cudaFuncSetAttribute(tau_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(tau_smem)));
+        int tau_per_sm = 0;
+        TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tau_per_sm, tau_kernel<Real>,
+                                                                kTauThreads, tau_smem));
+        if (tau_per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel tile");
+        const uint64_t groups = (g->num_forward + 31) / 32;
+        const uint64_t tau_blocks = std::max<uint64_t>(1, std::min<uint64_t>(
+            (groups + kTauThreads / 32 - 1) / (kTauThreads / 32), uint64_t(g->num_sms) * tau_per_sm));
         ScopedKernel k(g->prof, s, "tau");
-        tau_kernel<Real><<<grid_cap(g->num_forward, kTauThreads, g->num_sms, 16), kTauThreads, 0, s>>>(
+        tau_kernel<Real><<<unsigned(tau_blocks), kTauThreads, tau_smem, s>>>(
             g->idx.as<uint32_t>(), g->adj.as<uint32_t>(), g->row_of.as<uint32_t>(),
             g->rev.as<uint32_t>(), g->forward.as<uint32_t>(), g->num_forward, vec, g->omega, omega,
             g->onep.as<double>(), g->onem.as<double>(), etab, g->etab.as<double>(), eps_half, m, c,
@@ -729,23 +1156,31 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         TGTP_LAUNCH_CHECK("tau_kernel");
     }
 
-    // source kernel: shared-memory residuals when four warps' vectors fit in a block
+    // source kernel.  Shared-memory tier: one warp per block, each with its residual vector and
+    // visited bitmap in shared memory (one-warp blocks give the finest occupancy steps).  Global
+    // tier (large n): 4 warps per block, vectors in HBM.  TGTP_PVEC_TIER=smem|global overrides.
     const size_t pv_bytes = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
-    const size_t vis_bytes = ((size_t((n + 31) / 32) * 4) + 15) & ~size_t(15);
-    const size_t per_warp = pv_bytes + vis_bytes;
-    const bool use_smem = per_warp * kSrcWarps <= size_t(200) * 1024;
-    const size_t smem = use_smem ? per_warp * kSrcWarps : 0;
+    const size_t vis_bytes = (size_t(n) + 15) & ~size_t(15);
+    const size_t per_warp = pv_bytes + vis_bytes + kAccBytes;
+    bool use_smem = per_warp <= size_t(112) * 1024;
+    if (const char* t = std::getenv("TGTP_PVEC_TIER")) {
+        if (std::string(t) == "global") use_smem = false;
+        else if (std::string(t) == "smem" && per_warp <= size_t(227) * 1024) use_smem = true;
+    }
+    const int wpb = use_smem ? 1 : 4;
+    const int threads = wpb * 32;
+    const size_t smem = use_smem ? per_warp * wpb : size_t(wpb) * kAccBytes;
     auto kern = use_smem ? source_kernel<Real, true> : source_kernel<Real, false>;
     TGTP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
-    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSrcThreads, smem));
+    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
     if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "source kernel does not fit on an SM");
     uint64_t blocks = uint64_t(g->num_sms) * per_sm;
-    blocks = std::min<uint64_t>(blocks, (n + kSrcWarps - 1) / kSrcWarps);
-    const uint64_t warps = blocks * kSrcWarps;
+    blocks = std::min<uint64_t>(blocks, (n + wpb - 1) / wpb);
+    const uint64_t warps = blocks * wpb;
     const size_t maxd = std::max<uint32_t>(g->max_degree, 1);
     size_t scratch = warps * (2 * size_t(n) * 4 + maxd * sizeof(WalkItem));
-    if (!use_smem) scratch += warps * (size_t(n) * sizeof(Real) + size_t((n + 31) / 32) * 4);
+    if (!use_smem) scratch += warps * (size_t(n) * sizeof(Real) + size_t(n)) + 64;
     g->scratch.reserve(scratch + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
     SourceParams<Real> p;
@@ -766,7 +1201,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     if (!use_smem) {
         p.pvec_g = reinterpret_cast<Real*>(base);
         base += warps * size_t(n) * sizeof(Real);
-        p.vis_g = reinterpret_cast<uint32_t*>(base);
+        p.vis_g = base;
     }
     p.smem_per_warp = per_warp;
     p.max_degree = uint32_t(maxd);
@@ -775,10 +1210,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.gamma = cfg.gamma;
     p.ell_out = nullptr;
     p.stats = stats;
+    p.adjd = g->adjd.as<uint2>();
     p.budget_ns = deadline_from_env();
     {
         ScopedKernel k(g->prof, s, "source");
-        kern<<<unsigned(blocks), kSrcThreads, smem, s>>>(p);
+        kern<<<unsigned(blocks), threads, smem, s>>>(p);
         TGTP_LAUNCH_CHECK("source_kernel");
     }
     {
@@ -876,6 +1312,7 @@ tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out) {
         out->fallback_bouquets = st[kStFallback];
         out->tau_iterations = st[kStTauIters];
         out->tau_ambiguous = st[kStTauAmbiguous];
+        for (int i = 0; i < 8; ++i) out->phase_cycles[i] = st[kStPhase0 + i];
     });
 }
 

@@ -116,6 +116,17 @@ __global__ void rev_kernel(const uint32_t* __restrict__ idx, const uint32_t* __r
     }
 }
 
+// adjd[pos] = (neighbour, neighbour's degree): one coalesced 8-byte load per pushed slot instead of
+// a load plus a dependent degree gather.
+__global__ void adjd_kernel(const uint32_t* __restrict__ adj, const uint32_t* __restrict__ deg,
+                            uint64_t m, uint2* __restrict__ adjd) {
+    for (uint64_t pos = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; pos < m;
+         pos += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t u = adj[pos];
+        adjd[pos] = make_uint2(u, deg[u]);
+    }
+}
+
 // forward slots (v >= u) are the tail of each sorted row; count them per row.
 __global__ void forward_count_kernel(const uint32_t* __restrict__ idx,
                                      const uint32_t* __restrict__ adj, uint64_t n,
@@ -219,6 +230,10 @@ void graph_prepare(tgtp_graph* g) {
                                                            g->rev.as<uint32_t>(),
                                                            g->sym_src.as<uint32_t>());
         TGTP_LAUNCH_CHECK("rev_kernel");
+        g->adjd.reserve(sizeof(uint2) * (m + 1));
+        adjd_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(adj, g->deg.as<uint32_t>(), m,
+                                                            g->adjd.as<uint2>());
+        TGTP_LAUNCH_CHECK("adjd_kernel");
     }
     // forward slot list
     DeviceBuffer cnt;

@@ -145,6 +145,7 @@ struct tgtp_graph {
     tgtp::DeviceBuffer rev;      // slot (u,v) -> lower_bound of u in row v
     tgtp::DeviceBuffer sym_src;  // slot q -> 1 + last slot p with rev[p] == q (0: none)
     tgtp::DeviceBuffer forward;  // slots with v >= u, in CSR order
+    tgtp::DeviceBuffer adjd;     // slot -> (neighbour, neighbour's degree)
 
     // eigenpairs
     uint32_t omega = 0;
