@@ -172,6 +172,12 @@ tgtp_status saba_count_static(const uint32_t* device_idx, const uint32_t* device
                               uint32_t depth, uint32_t n_walks, void* cuda_stream,
                               saba_result* out);
 
+/* ---- memory ---------------------------------------------------------------------------------- */
+/* Device blocks of released graphs are kept for reuse (creating a graph per input would otherwise
+ * pay cudaMalloc/cudaFree for its scratch every time).  This returns every cached block to the
+ * driver; blocks held by live graphs are unaffected. */
+tgtp_status tgtp_release_cached_memory(void);
+
 /* ---- profiling ------------------------------------------------------------------------------ */
 /* When on, every kernel launch is bracketed by CUDA events on the handle's stream and its device
  * time is accumulated per kernel name.  Turning it on clears the table. */

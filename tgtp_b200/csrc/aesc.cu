@@ -519,15 +519,13 @@ source_kernel(SourceParams<Real> p) {
         const Real ds = from_u64<Real>(dsi);
         // preds = 1.0 / ds (:468-470); stored together with the first round's update below
         const Real pinit = from_f64<Real>(__ddiv_rn(1.0, double(ds)));
-        if (lane == 0) {
-            pvec[src] = Real(1);
-            q[0] = src;
-        }
-        uint32_t qs = 1;
+        uint32_t qs = 0;
         int ell = 0;
         Real gmin, gmax;
         bool timed_out = false;
-        // row loaders (slot id, neighbour, tau) for the pipelined passes over the source's row
+        unsigned long long pcost = 0;
+        Real mx = Real(0), mn = Real(1);
+        // row loaders (neighbour, tau) for the pipelined passes over the source's row
         auto load_adj = [&](uint32_t c, uint32_t* r) {
 #pragma unroll
             for (int b = 0; b < kB; ++b) {
@@ -542,9 +540,78 @@ source_kernel(SourceParams<Real> p) {
                 r[b] = o < dsi ? __ldg(taus + rb + o) : 0;
             }
         };
-        __syncwarp();
         lap(0);
+        // ---- round 1 in closed form (:457-503, first pass of the loop) ----
+        // The frontier is {src} with residual 1 (pvec[src] = 1.0, then zeroed as it is drained):
+        // every neighbour u is discovered in row order and receives 0 + 1/deg(u) = 1/deg(u), so
+        // the round's new frontier, residuals, degree sum, max / min and row update
+        // preds = 1/ds + (0 - 1/deg(u)) / ds follow from one pass over the row.  Neighbours are
+        // distinct (tgtp_run rejects repeated neighbours and self-loops).
+        pipelined<uint2>(dsi,
+            [&](uint32_t c, uint2* r) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    const uint32_t o = c + 32 * b + lane;
+                    r[b] = o < dsi ? __ldg(p.adjd + rb + o) : make_uint2(NONE, 1u);
+                }
+            },
+            [&](uint32_t c, const uint2* r) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    if (r[b].x == NONE) continue;
+                    const uint32_t o = c + 32 * b + lane;
+                    const Real pu = rdiv(Real(1), from_u64<Real>(r[b].y));
+                    pvec[r[b].x] = pu;
+                    qn[o] = r[b].x;
+                    pcost += r[b].y;
+                    mx = std_max(mx, pu);
+                    mn = std_min(mn, pu);
+                    p.preds[rb + o] = radd(pinit, rdiv(rsub(Real(0), pu), ds));
+                }
+            });
+        st_pv += 1;
+        st_tr += dsi;
+        qs = dsi;
+        ell = 1;
+        { uint32_t* tmp = q; q = qn; qn = tmp; }
+        __syncwarp();
+        lap(1);
         while (true) {
+            // ---- the push/walk cost test (:483-502) ----
+            const double picost = double(warp_sum_u64(pcost));
+            gmax = warp_max(mx);
+            gmin = warp_min(mn);
+            gmin = qs < n ? Real(0) : gmin;
+            const double dse0 = __dmul_rn(double(ds), p.eps);
+            const double dse2 = __dmul_rn(dse0, dse0);
+            double rw = 0;
+            pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
+#pragma unroll
+                for (int b = 0; b < kB; ++b) {
+                    const uint32_t o = c + 32 * b + lane;
+                    const int rest = tv[b] - ell;
+                    double nrd = 0;
+                    const bool has = o < dsi && rest > 0;
+                    if (has) {
+                        const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
+                                                     __dsub_rn(double(gmax), double(gmin)));
+                        const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
+                        nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
+                    }
+                    unsigned hb = __ballot_sync(kFullMask, has);
+                    while (hb) {  // rwcost += nr in slot order
+                        const int l = __ffs(hb) - 1;
+                        hb &= hb - 1;
+                        rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
+                    }
+                }
+            });
+            lap(3);
+            if (picost >= __dmul_rn(25.0, rw)) break;
+            if (globaltimer_ns() > deadline) {
+                timed_out = true;
+                break;
+            }
             // ---- diffuse (:218-239) ----
             // The frontier is drained in order, one vertex at a time; the lanes share the
             // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
@@ -554,7 +621,7 @@ source_kernel(SourceParams<Real> p) {
             // new frontier's degree sum) is summed on discovery.  Every vertex has at least one
             // chunk: tgtp_run rejects isolated vertices.
             uint32_t qns = 0;
-            unsigned long long pcost = 0;
+            pcost = 0;
             st_pv += qs;
             for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
                 uint32_t myv = 0, myb = 0, myd = 0;
@@ -664,7 +731,8 @@ source_kernel(SourceParams<Real> p) {
             }
             // clear the new frontier's flags and take its residual max / min (:484-491; max and
             // min do not depend on order)
-            Real mx = Real(0), mn = Real(1);
+            mx = Real(0);
+            mn = Real(1);
             pipelined<uint32_t>(qns,
                 [&](uint32_t i0, uint32_t* r) {
 #pragma unroll
@@ -688,41 +756,6 @@ source_kernel(SourceParams<Real> p) {
             qs = qns;
             ++ell;
             lap(2);
-            // ---- the push/walk cost test (:483-502) ----
-            const double picost = double(warp_sum_u64(pcost));
-            gmax = warp_max(mx);
-            gmin = warp_min(mn);
-            gmin = qs < n ? Real(0) : gmin;
-            const double dse0 = __dmul_rn(double(ds), p.eps);
-            const double dse2 = __dmul_rn(dse0, dse0);
-            double rw = 0;
-            pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
-#pragma unroll
-                for (int b = 0; b < kB; ++b) {
-                    const uint32_t o = c + 32 * b + lane;
-                    const int rest = tv[b] - ell;
-                    double nrd = 0;
-                    const bool has = o < dsi && rest > 0;
-                    if (has) {
-                        const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
-                                                     __dsub_rn(double(gmax), double(gmin)));
-                        const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
-                        nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
-                    }
-                    unsigned hb = __ballot_sync(kFullMask, has);
-                    while (hb) {  // rwcost += nr in slot order
-                        const int l = __ffs(hb) - 1;
-                        hb &= hb - 1;
-                        rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
-                    }
-                }
-            });
-            lap(3);
-            if (picost >= __dmul_rn(25.0, rw)) break;
-            if (globaltimer_ns() > deadline) {
-                timed_out = true;
-                break;
-            }
         }
         if (timed_out) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);

@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <memory>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -18,6 +20,104 @@ thread_local std::string g_last_error;
 }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// ---- device block cache and stream pool -----------------------------------------------------------
+namespace {
+std::mutex g_cache_mu;
+std::map<std::pair<int, size_t>, std::vector<void*>> g_free_blocks;  // (device, class) -> blocks
+std::map<int, std::vector<cudaStream_t>> g_free_streams;
+
+size_t size_class(size_t bytes) {
+    if (bytes <= (size_t(1) << 20)) {  // powers of two up to 1 MiB
+        size_t c = 256;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+    const size_t g = size_t(2) << 20;  // 2 MiB steps above
+    return (bytes + g - 1) / g * g;
+}
+}  // namespace
+
+void* cache_alloc(size_t bytes, size_t* granted) {
+    int dev = 0;
+    TGTP_CUDA(cudaGetDevice(&dev));
+    const size_t c = size_class(bytes);
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        auto it = g_free_blocks.find({dev, c});
+        if (it != g_free_blocks.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            *granted = c;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, c);
+    if (e == cudaErrorMemoryAllocation) {  // give the cache back to the driver and retry once
+        (void)cudaGetLastError();
+        cache_trim();
+        e = cudaMalloc(&p, c);
+    }
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? TGTP_ERR_OUT_OF_MEMORY : TGTP_ERR_CUDA,
+             std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    *granted = c;
+    return p;
+}
+
+void cache_free(void* p, size_t granted) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_free_blocks[{dev, granted}].push_back(p);
+}
+
+void cache_trim() {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto& kv : g_free_blocks) {
+        cudaSetDevice(kv.first.first);
+        for (void* p : kv.second) cudaFree(p);
+        kv.second.clear();
+    }
+    cudaSetDevice(cur);
+}
+
+cudaStream_t stream_acquire() {
+    int dev = 0;
+    TGTP_CUDA(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        auto& v = g_free_streams[dev];
+        if (!v.empty()) {
+            cudaStream_t s = v.back();
+            v.pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    TGTP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+void stream_release(cudaStream_t s) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaStreamDestroy(s);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_free_streams[dev].push_back(s);
+}
 
 // ---- profiler ------------------------------------------------------------------------------------
 cudaEvent_t Profiler::take() {
@@ -257,10 +357,10 @@ void graph_prepare(tgtp_graph* g) {
 }  // namespace tgtp
 
 tgtp_graph::~tgtp_graph() {
-    if (own_stream) {
-        cudaStreamSynchronize(own_stream);
-        cudaStreamDestroy(own_stream);
-    }
+    // the device buffers (members) are returned to the cache after this body, once the device
+    // is idle; the stream goes back to the pool
+    if (stream) cudaStreamSynchronize(stream);
+    if (own_stream) tgtp::stream_release(own_stream);
 }
 
 using namespace tgtp;
@@ -308,7 +408,7 @@ tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t
         g->has_multi_edges = multi;
         TGTP_CUDA(cudaGetDevice(&g->device));
         TGTP_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
-        TGTP_CUDA(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+        g->own_stream = stream_acquire();
         g->stream = g->own_stream;
         g->idx.reserve(sizeof(uint32_t) * (n + 1));
         g->adj.reserve(sizeof(uint32_t) * (m + 1));
@@ -471,6 +571,10 @@ tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t
         if ((unsigned __int128)sums[0] != expect)
             fail(TGTP_ERR_OVERFLOW, "a uint32 visit counter overflowed");
     });
+}
+
+tgtp_status tgtp_release_cached_memory(void) {
+    return guarded([&] { cache_trim(); });
 }
 
 tgtp_status tgtp_graph_set_profiling(tgtp_graph* g, int enable) {

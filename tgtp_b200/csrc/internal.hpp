@@ -61,6 +61,18 @@ tgtp_status guarded(F&& f) {
     }
 }
 
+// Process-wide cache of device blocks.  Graphs are created and released often (one per input in a
+// batch, one per call through the plain C entry points), and cudaMalloc / cudaFree of the ~100 MB
+// of per-run scratch would dominate such calls.  Blocks are rounded to a size class and kept per
+// device after release; a release first waits for the device to be idle, so no queued kernel can
+// still be using the block when it is handed out again.  tgtp_release_cached_memory() returns the
+// cached blocks to the driver.
+void* cache_alloc(size_t bytes, size_t* granted);
+void cache_free(void* p, size_t granted);
+void cache_trim();
+cudaStream_t stream_acquire();
+void stream_release(cudaStream_t s);
+
 // Grow-only device allocation owned by a graph handle.
 struct DeviceBuffer {
     void* ptr = nullptr;
@@ -70,7 +82,7 @@ struct DeviceBuffer {
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
     ~DeviceBuffer() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) cache_free(ptr, bytes);
         ptr = nullptr;
         bytes = 0;
     }
@@ -78,8 +90,7 @@ struct DeviceBuffer {
         if (want <= bytes && ptr) return;
         release();
         if (want == 0) want = 16;
-        TGTP_CUDA(cudaMalloc(&ptr, want));
-        bytes = want;
+        ptr = cache_alloc(want, &bytes);
     }
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
