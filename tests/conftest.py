@@ -6,6 +6,7 @@ from __future__ import annotations
 import json
 import os
 import sys
+import tempfile
 
 import numpy as np
 import pytest
@@ -74,3 +75,18 @@ def golden_tgtp_case(manifest, name):
 
 def load_golden_scores(run):
     return np.load(os.path.join(GOLDEN, "tgtp", run["scores"]))
+
+
+@pytest.fixture(scope="session")
+def config1_inputs():
+    """Chung-Lu n=4,039 with 128 eigenpairs written and parsed back like the reference's files."""
+    from tgtp_b200 import eigenprep, synth
+    from tgtp_b200.aesc import load_eigens_txt
+
+    g = synth.config1_graph(1)
+    d = tempfile.mkdtemp(prefix="tgtp_cfg1_")
+    synth.write_graph_txt(g, os.path.join(d, "graph.txt"))
+    path = eigenprep.eigenprep_folder(d, 128)
+    idx, adj = g.csr()
+    values, v32, v64 = load_eigens_txt(path, g.n, 128)
+    return dict(idx=idx, adj=adj, values=values, v32=v32, v64=v64, n=g.n)

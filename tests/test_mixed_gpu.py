@@ -1,0 +1,82 @@
+"""The MIXED form on the GPU: FP32 residuals and lane-parallel compensated FP32 eigen projections
+(F32 or BF16 storage), FP64 tau bounds / stop test / score accumulation, frontier-parallel push.
+It is not bit-exact with the reference by design; it must be deterministic, symmetric and as
+accurate against exact spanning centrality (oracle/exact_sc.py) as the FP64 form."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_tgtp_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(c):
+    from tgtp_b200.aesc import VEC_BF16, VEC_F32, VEC_F64, AESCGraph
+
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    g.upload_eigens(c["values"], c["v32"], VEC_BF16)
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    return g
+
+
+def _rev(idx, adj):
+    rows = np.repeat(np.arange(len(idx) - 1), np.diff(idx.astype(np.int64)))
+    key = rows.astype(np.int64) * len(idx) + adj
+    order = np.argsort(key)
+    return order[np.searchsorted(key[order], adj.astype(np.int64) * len(idx) + rows)]
+
+
+@pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
+def test_mixed_deterministic_symmetric_and_as_accurate_as_fp64(manifest, cuda_device, name):
+    from oracle import exact_sc
+    from tgtp_b200.aesc import (AESC, AESCConfig, PRECISION_FP64, PRECISION_MIXED, VEC_BF16,
+                                VEC_F32)
+
+    c = golden_tgtp_case(manifest, name)
+    g = _graph(c)
+    exact = exact_sc.exact_scores(c["idx"], c["adj"])
+    rev = _rev(c["idx"], c["adj"])
+    for run in c["runs"]:
+        eps, gamma = run["epsilon"], run["gamma"]
+        f64 = AESC(g, AESCConfig(eps, omega=c["omega"], gamma=gamma, precision=PRECISION_FP64)).tgtp()
+        acc64 = exact_sc.accuracy(f64, exact, eps)
+        for vd in (VEC_F32, VEC_BF16):
+            a = AESC(g, AESCConfig(eps, omega=c["omega"], gamma=gamma, precision=PRECISION_MIXED,
+                                   vec_dtype=vd))
+            s1, s2 = a.tgtp(), a.tgtp()
+            assert np.array_equal(s1.view(np.uint32), s2.view(np.uint32)), "not deterministic"
+            assert np.all(np.isfinite(s1)) and np.array_equal(s1, s1[rev])
+            accm = exact_sc.accuracy(s1, exact, eps)
+            # as accurate as the FP64 form against the exact scores: (almost) as many slots within
+            # epsilon, or no larger maximum and mean error (graphs where the bound's mixing
+            # assumption fails, like odd cycles, put few slots of either form within epsilon)
+            as_many = accm["fraction_within_epsilon"] >= acc64["fraction_within_epsilon"] - 0.01
+            no_worse = (accm["max_absolute_error"] <= acc64["max_absolute_error"] * (1 + 1e-6) and
+                        accm["mean_absolute_error"] <= acc64["mean_absolute_error"] * (1 + 1e-6))
+            assert as_many or no_worse, (run, vd, accm, acc64)
+            assert accm["max_absolute_error"] <= max(2 * acc64["max_absolute_error"], eps), (
+                run, vd, accm, acc64)
+    g.free()
+
+
+def test_mixed_matches_fp64_when_no_walks_run(cuda_device, config1_inputs):
+    """With one push round and no walks (epsilon 0.05 on the 4,039-vertex graph) the forms differ
+    only by rounding: FP32 residuals and FP32 projections against FP64."""
+    from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_FP64, PRECISION_MIXED,
+                                VEC_BF16, VEC_F32, VEC_F64)
+
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    g.upload_eigens(c["values"], c["v32"], VEC_BF16)
+    f64 = AESC(g, AESCConfig(0.05, precision=PRECISION_FP64)).tgtp()
+    for vd in (VEC_F32, VEC_BF16):
+        a = AESC(g, AESCConfig(0.05, precision=PRECISION_MIXED, vec_dtype=vd))
+        mixed = a.tgtp()
+        assert a.stats()["walk_edges"] == 0
+        np.testing.assert_allclose(mixed, f64, rtol=1e-5, atol=0)
+    g.free()

@@ -6,9 +6,6 @@ FP64 form: bit-exact with the oracle's FP64 restatement (same operations, same o
 Work counters (push rounds, traversals, walks, fallbacks) equal the oracle's."""
 from __future__ import annotations
 
-import os
-import tempfile
-
 import numpy as np
 import pytest
 
@@ -82,21 +79,6 @@ def test_fp64_matches_oracle_and_reference(manifest, cuda_device, oracle_lib, na
         tol = np.maximum(1e-6 * np.abs(want), 2 * np.spacing(np.abs(want)))
         assert (np.abs(got.astype(np.float64) - want) > tol).mean() <= 0.01
     g.free()
-
-
-@pytest.fixture(scope="module")
-def config1_inputs():
-    """Chung-Lu n=4,039 with 128 eigenpairs written and parsed back like the reference's files."""
-    from tgtp_b200 import eigenprep, synth
-    from tgtp_b200.aesc import load_eigens_txt
-
-    g = synth.config1_graph(1)
-    d = tempfile.mkdtemp(prefix="tgtp_cfg1_")
-    synth.write_graph_txt(g, os.path.join(d, "graph.txt"))
-    path = eigenprep.eigenprep_folder(d, 128)
-    idx, adj = g.csr()
-    values, v32, v64 = load_eigens_txt(path, g.n, 128)
-    return dict(idx=idx, adj=adj, values=values, v32=v32, v64=v64, n=g.n)
 
 
 @pytest.mark.parametrize("eps", [0.05, 0.01, 0.005])

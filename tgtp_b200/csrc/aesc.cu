@@ -39,7 +39,7 @@ constexpr int kPushAhead = 4;         // adjacency chunks loaded ahead in the pu
 constexpr int kB = 4;                 // 32-wide chunks per pipelined load step
 constexpr int kTopK = 16;            // register top-k used for gamma <= 16
 // per-warp shared scratch of the chi step: 64 u64 max/min images + 33 + 32 u32 slot offsets
-constexpr size_t kAccBytes = 1024;
+constexpr size_t kAccBytes = 1280;
 constexpr int kTauTableRows = 64;    // rows of the eigen_t_1 power table (api.cu)
 constexpr uint64_t kMaxWalks = 0xffffffffull;  // nr beyond the 32-bit grid is not supported
 
@@ -274,25 +274,209 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
     }
 }
 
+// ---- stage 1 (mixed form): tau with lane-parallel, compensated FP32 projections ---------------
+// d_i^2 = (x_u[i] - x_v[i])^2 and the weighted terms d_i^2 (1 + lambda_i) and
+// d_i^2 lambda_i^(2(k+1)) / (1 - lambda_i) are formed in FP32 from F32 or BF16 eigenvectors; the
+// bound itself (get_tau: logs, ceil, odd rounding, the delta iteration) is evaluated in FP64.
+
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+
+__device__ __forceinline__ float vec_load(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float vec_load(const __nv_bfloat16* p) {
+    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p))));
+}
+
+// get_tau (src/aesc.h:129-135) in FP64 for the mixed form (no bit-level parity asked): the degree
+// terms from reciprocals, one division and the precomputed 1 / log(1/|lambda|).
+__device__ __forceinline__ int get_tau_mixed(double inv1, double inv2, double epsilon,
+                                             double one_m_lam2, double inv_b, double delta,
+                                             double ups) {
+    const double ed = epsilon - delta;
+    const double eps_delta = ed > 0.0 ? ed : epsilon;
+    const double x = (inv2 + inv1) - 2.0 * inv2 * inv1 - ups;
+    const double a = log(std_max(x / (eps_delta * one_m_lam2), 1.0));
+    const int tau = x86_f64_to_i32(std_max(ceil(a * inv_b - 1.0), 1.0));
+    return tau % 2 == 0 ? tau + 1 : tau;
+}
+
+// Weight of index i in delta_k (mixed form): lambda_i^(2(k+1)) / (1 - lambda_i) in FP32, zero at the
+// indices the reference leaves out; beyond the precomputed rows the FP64 power chain continues.
+__device__ __forceinline__ float mixed_weight(const float* __restrict__ mixc,
+                                              const double* __restrict__ etabd,
+                                              const double* __restrict__ onem, uint32_t stride,
+                                              uint32_t omega, uint32_t k, uint32_t i) {
+    if (i < 1 || i + 1 >= omega) return 0.f;
+    if (k < uint32_t(kTauTableRows)) return __ldg(mixc + size_t(k + 1) * omega + i);
+    double ev = __ldg(etabd + size_t(kTauTableRows - 1) * stride + i);
+    const double sq = __ldg(etabd + i);
+    for (uint32_t r = kTauTableRows - 1; r < k; ++r) ev *= sq;
+    return float(ev / __ldg(onem + i));
+}
+
+// Error-free combination of the eight partial sums of a lane group (TwoSum tree, the rounding
+// errors carried and added back).
+__device__ __forceinline__ double group_reduce(float a) {
+    float ca = 0.f;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        const float a2 = __shfl_xor_sync(kFullMask, a, o);
+        const float ca2 = __shfl_xor_sync(kFullMask, ca, o);
+        float t, e;
+        two_sum(a, a2, t, e);
+        a = t;
+        ca = __fadd_rn(__fadd_rn(ca, ca2), e);
+    }
+    return double(a) + double(ca);
+}
+
+// The mixed tau kernel.  A warp works on 32 forward slots at a time, four at once: the 8 lanes of
+// group g take slot 4 s + g at step s and hold indices i = l, l + 8, ... of its two eigen rows
+// (32-byte row pieces per group).  Each lane accumulates its terms d_i^2 w_i with FMAs (the terms are
+// non-negative, so a lane's sum has relative error below 16 ulp); the group's eight partial sums
+// are combined by group_reduce.  The slot's sums land in lane 4 s + g, and every lane then
+// evaluates its own slot's bound in FP64 at once.
+template <class Vec>
+__global__ void __launch_bounds__(256)
+tau_mixed_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
+                 const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ rev,
+                 const uint32_t* __restrict__ forward, uint64_t num_forward,
+                 const Vec* __restrict__ vec, uint32_t stride, uint32_t omega,
+                 const float* __restrict__ mixc, const double* __restrict__ etabd,
+                 const double* __restrict__ onem, double eps_half, double mdbl, TauConst c,
+                 int* __restrict__ taus, unsigned long long* __restrict__ stats) {
+    extern __shared__ __align__(16) unsigned char msm[];
+    float2* w01 = reinterpret_cast<float2*>(msm);  // (1 + lambda_i, delta_0 weight of index i)
+    for (uint32_t i = threadIdx.x; i < omega; i += blockDim.x)
+        w01[i] = make_float2(__ldg(mixc + i), __ldg(mixc + omega + i));
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, grp = lane >> 3, sl = lane & 7;
+    const uint64_t gw = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const double inv_b1 = 1.0 / c.b1, inv_b2 = 1.0 / c.b2;
+    unsigned long long iters = 0;
+    for (uint64_t base = gw * 32; base < num_forward; base += nw * 32) {
+        const uint64_t e = base + lane;
+        const bool act = e < num_forward;
+        uint32_t pos = 0, u = 0, v = 0, du = 1, dv = 1;
+        if (act) {
+            pos = __ldg(forward + e);
+            u = __ldg(row_of + pos);
+            v = __ldg(adj + pos);
+            du = __ldg(idx + u + 1) - __ldg(idx + u);
+            dv = __ldg(idx + v + 1) - __ldg(idx + v);
+        }
+        double ups = 0, del = 0;
+        for (uint32_t st = 0; st < 8; ++st) {
+            const uint32_t t = st * 4 + grp;
+            const Vec* ur = vec + size_t(__shfl_sync(kFullMask, u, t)) * stride;
+            const Vec* vr = vec + size_t(__shfl_sync(kFullMask, v, t)) * stride;
+            float a = 0.f, b = 0.f;
+#pragma unroll 4
+            for (uint32_t i = sl; i < omega; i += 8) {
+                const float d = vec_load(ur + i) - vec_load(vr + i);
+                const float d2 = d * d;
+                const float2 wi = w01[i];
+                a = __fmaf_rn(d2, wi.x, a);
+                b = __fmaf_rn(d2, wi.y, b);
+            }
+            const double s1 = group_reduce(a), s2 = group_reduce(b);
+            const uint32_t from = (lane & 3) * 8;  // lane 4 st + g takes group g's sums
+            const double r1 = __shfl_sync(kFullMask, s1, from);
+            const double r2 = __shfl_sync(kFullMask, s2, from);
+            if ((lane >> 2) == st) {
+                ups = r1 / mdbl;
+                del = r2 / mdbl;
+            }
+        }
+        const double inv1 = 1.0 / double(du), inv2 = 1.0 / double(dv);
+        int tau = 0, tsteps = 1;
+        uint32_t k = 0;
+        bool need = false;
+        if (act) {
+            tau = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l1sq, inv_b1, 0.0, 0.0);
+            ++iters;
+            const int tp = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l2sq, inv_b2, del, ups);
+            if (tsteps <= tp && tp < tau) {
+                tau = tp;
+                tsteps += 2;
+                k = 1;
+                need = true;
+            }
+        }
+        // further delta iterations (:191-204) for slots that still improve, four at a time
+        while (true) {
+            unsigned nb = __ballot_sync(kFullMask, need);
+            if (!nb) break;
+            while (nb) {
+                int sel[4];
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    sel[g] = nb ? __ffs(nb) - 1 : -1;
+                    if (nb) nb &= nb - 1;
+                }
+                const uint32_t tt = sel[grp] < 0 ? 0u : uint32_t(sel[grp]);
+                const Vec* ur = vec + size_t(__shfl_sync(kFullMask, u, tt)) * stride;
+                const Vec* vr = vec + size_t(__shfl_sync(kFullMask, v, tt)) * stride;
+                const uint32_t kt = __shfl_sync(kFullMask, k, tt);
+                float b = 0.f;
+                for (uint32_t i = sl; i < omega; i += 8) {
+                    const float d = vec_load(ur + i) - vec_load(vr + i);
+                    b = __fmaf_rn(d * d, mixed_weight(mixc, etabd, onem, stride, omega, kt, i), b);
+                }
+                const double dk = group_reduce(b);
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    const double r = __shfl_sync(kFullMask, dk, g * 8);
+                    if (sel[g] >= 0 && lane == uint32_t(sel[g])) del = r / mdbl;
+                }
+            }
+            if (need) {
+                ++iters;
+                const int tp = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l2sq, inv_b2, del, ups);
+                if (tsteps <= tp && tp < tau) {
+                    tau = tp;
+                    tsteps += 2;
+                    ++k;
+                } else {
+                    need = false;
+                }
+            }
+        }
+        if (act) {
+            taus[pos] = tau;
+            taus[__ldg(rev + pos)] = tau;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) iters += __shfl_xor_sync(kFullMask, iters, o);
+    if (lane == 0 && iters) atomicAdd(stats + kStTauIters, iters);
+}
+
 // ---- stage 2: per-source push, edge bound and walks -----------------------------------------------
 struct WalkItem {
     uint32_t pos, v, len, pad;
     unsigned long long nr;
 };
 
-template <class Real>
+template <class Real, class Acc>
 struct SourceParams {
     const uint32_t* idx;
     const uint32_t* adj;
     const uint32_t* deg;
     uint32_t n;
     const int* taus;
-    Real* preds;
+    Acc* preds;           // pre-symmetric row scores (Real in the parity forms, double in MIXED)
     unsigned* work;       // [0] next source, [1] error flags
     uint32_t* qbuf;       // 2 * n per warp
     WalkItem* items;      // max_degree per warp
     Real* pvec_g;         // n per warp (global tier)
-    unsigned char* vis_g; // n per warp (global tier)
+    Real* rbuf;           // n per warp: frontier residuals taken together (Jacobi push)
+    unsigned char* vis_g; // vis_stride per warp (global tier)
+    size_t vis_stride;
     size_t smem_per_warp;
     uint32_t max_degree;
     double eps;
@@ -335,6 +519,17 @@ __device__ __forceinline__ void pipelined(uint32_t count, Load load, Proc proc) 
         proc(i0, a);
 #pragma unroll
         for (int k = 0; k < kB; ++k) a[k] = b[k];
+    }
+}
+
+// preds[pos] += (pvec[src] - pvec[w]) / ds (:236): in the row's own real type in the parity forms,
+// accumulated in FP64 in the mixed form.
+template <class Real, class Acc>
+__device__ __forceinline__ Acc row_update(Acc old, Real ps, Real pv, Real ds) {
+    if constexpr (std::is_same<Real, Acc>::value) {
+        return radd(old, rdiv(rsub(ps, pv), ds));
+    } else {
+        return __dadd_rn(old, __ddiv_rn(__dsub_rn(double(ps), double(pv)), double(ds)));
     }
 }
 
@@ -453,9 +648,9 @@ __device__ __forceinline__ void seg_maxmin(uint32_t seg, Real& mx, Real& mn) {
     }
 }
 
-template <class Real, bool SMEM>
+template <class Real, class Acc, bool SMEM, bool JACOBI>
 __global__ void __launch_bounds__(kSrcMaxThreads)
-source_kernel(SourceParams<Real> p) {
+source_kernel(SourceParams<Real, Acc> p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wib = threadIdx.x >> 5;
@@ -475,7 +670,7 @@ source_kernel(SourceParams<Real> p) {
         acc = reinterpret_cast<unsigned long long*>(base + pv + ((size_t(n) + 15) & ~size_t(15)));
     } else {
         pvec = p.pvec_g + gw * size_t(n);
-        vis = p.vis_g + gw * size_t(n);
+        vis = p.vis_g + gw * p.vis_stride;
         acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
     for (uint32_t i = lane; i < n; i += 32) {
@@ -518,7 +713,7 @@ source_kernel(SourceParams<Real> p) {
         const uint32_t dsi = re - rb;
         const Real ds = from_u64<Real>(dsi);
         // preds = 1.0 / ds (:468-470); stored together with the first round's update below
-        const Real pinit = from_f64<Real>(__ddiv_rn(1.0, double(ds)));
+        const Acc pinit = from_f64<Acc>(__ddiv_rn(1.0, double(ds)));
         uint32_t qs = 0;
         int ell = 0;
         Real gmin, gmax;
@@ -566,7 +761,7 @@ source_kernel(SourceParams<Real> p) {
                     pcost += r[b].y;
                     mx = std_max(mx, pu);
                     mn = std_min(mn, pu);
-                    p.preds[rb + o] = radd(pinit, rdiv(rsub(Real(0), pu), ds));
+                    p.preds[rb + o] = row_update<Real, Acc>(pinit, Real(0), pu, ds);
                 }
             });
         st_pv += 1;
@@ -612,6 +807,10 @@ source_kernel(SourceParams<Real> p) {
                 timed_out = true;
                 break;
             }
+            uint32_t qns = 0;
+            pcost = 0;
+            st_pv += qs;
+            if constexpr (!JACOBI) {
             // ---- diffuse (:218-239) ----
             // The frontier is drained in order, one vertex at a time; the lanes share the
             // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
@@ -620,9 +819,7 @@ source_kernel(SourceParams<Real> p) {
             // one coalesced 8-byte load per lane, issued kPushAhead chunks before use.  picost (the
             // new frontier's degree sum) is summed on discovery.  Every vertex has at least one
             // chunk: tgtp_run rejects isolated vertices.
-            uint32_t qns = 0;
-            pcost = 0;
-            st_pv += qs;
+
             for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
                 uint32_t myv = 0, myb = 0, myd = 0;
                 if (i0 + lane < qs) {
@@ -698,6 +895,117 @@ source_kernel(SourceParams<Real> p) {
                     }
                 }
             }
+            } else {
+                // ---- Jacobi push (mixed form) ----
+                // The frontier's residuals are taken together (r_i = pvec[q_i], pvec[q_i] = 0),
+                // then pushed over the concatenated adjacency of 32 frontier vertices at a time:
+                // each lane walks entries lane, lane + 32, ... with a cursor over the vertices'
+                // start offsets.  Two lanes of one step that reach the same neighbour apply their
+                // shares one after the other in lane order, so the result is deterministic.
+
+                pipelined<uint32_t>(qs,
+                    [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            r[b] = i < qs ? q[i] : NONE;
+                        }
+                    },
+                    [&](uint32_t i0, const uint32_t* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            if (r[b] == NONE) continue;
+                            p.rbuf[gw * size_t(n) + i0 + 32 * b + lane] = pvec[r[b]];
+                            pvec[r[b]] = Real(0);
+                        }
+                    });
+                __syncwarp();
+                uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64);
+                uint32_t* vbs = exs + 33;
+                Real* rvs = reinterpret_cast<Real*>(vbs + 32);
+                for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
+                    uint32_t vb = 0, vd = 0;
+                    Real rv = Real(0);
+                    if (i0 + lane < qs) {
+                        const uint32_t v = q[i0 + lane];
+                        vb = __ldg(idx + v);
+                        vd = __ldg(idx + v + 1) - vb;
+                        rv = p.rbuf[gw * size_t(n) + i0 + lane];
+                    }
+                    uint32_t incl = vd;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                        if (lane >= uint32_t(o)) incl += y;
+                    }
+                    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                    exs[lane] = incl - vd;
+                    vbs[lane] = vb;
+                    rvs[lane] = rv;
+                    if (lane == 31) exs[32] = total;
+                    __syncwarp();
+                    st_tr += total;
+                    uint32_t cm = 0;
+                    struct PEnt {
+                        uint32_t seg, u, du;
+                    };
+                    pipelined<PEnt>(total,
+                        [&](uint32_t e0, PEnt* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const uint32_t e = e0 + 32 * b + lane;
+                                r[b].seg = 32u;
+                                r[b].u = NONE;
+                                r[b].du = 1u;
+                                if (e < total) {
+                                    while (exs[cm + 1] <= e) ++cm;
+                                    const uint2 a = __ldg(p.adjd + vbs[cm] + (e - exs[cm]));
+                                    r[b].seg = cm;
+                                    r[b].u = a.x;
+                                    r[b].du = a.y;
+                                }
+                            }
+                        },
+                        [&](uint32_t, const PEnt* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const bool valid = r[b].seg < 32u;
+                                const uint32_t u = r[b].u;
+                                const Real share = valid ? rvs[r[b].seg] / from_u64<Real>(r[b].du) : Real(0);
+                                // entries of one frontier vertex are distinct neighbours; only a
+                                // step that spans several vertices can repeat one
+                                const uint32_t seg0 = __shfl_sync(kFullMask, r[b].seg, 0);
+                                const bool one_seg = __all_sync(kFullMask, !valid || r[b].seg == seg0);
+                                const unsigned grp =
+                                    one_seg ? (1u << lane) : __match_any_sync(kFullMask, u);
+                                const bool unique =
+                                    one_seg || __all_sync(kFullMask, !valid || grp == (1u << lane));
+                                if (unique) {
+                                    if (valid) pvec[u] = pvec[u] + share;
+                                } else {
+                                    for (uint32_t l = 0; l < 32; ++l) {
+                                        if (lane == l && valid) pvec[u] = pvec[u] + share;
+                                        __syncwarp();
+                                    }
+                                }
+                                const bool leader = valid && lane == uint32_t(__ffs(grp) - 1);
+                                bool fresh = false;
+                                if (leader && vis[u] == 0) {
+                                    vis[u] = 1;
+                                    fresh = true;
+                                }
+                                const unsigned bal = __ballot_sync(kFullMask, fresh);
+                                if (fresh) {
+                                    qn[qns + __popc(bal & lt)] = u;
+                                    pcost += r[b].du;
+                                }
+                                qns += __popc(bal);
+                                __syncwarp();
+                            }
+                        });
+                    __syncwarp();
+                }
+            }
             __syncwarp();
             lap(1);
             // preds[row] += (pvec[src] - pvec[adj]) / ds (:235-237); the first round adds to the
@@ -706,7 +1014,7 @@ source_kernel(SourceParams<Real> p) {
                 const Real ps = pvec[src];
                 struct SlotPred {
                     uint32_t w;
-                    Real old;
+                    Acc old;
                 };
                 pipelined<SlotPred>(dsi,
                     [&](uint32_t c, SlotPred* r) {
@@ -726,7 +1034,7 @@ source_kernel(SourceParams<Real> p) {
                         for (int b = 0; b < kB; ++b)
                             if (r[b].w != NONE)
                                 p.preds[rb + c + 32 * b + lane] =
-                                    radd(r[b].old, rdiv(rsub(ps, pvec[r[b].w]), ds));
+                                    row_update<Real, Acc>(r[b].old, ps, pvec[r[b].w], ds);
                     });
             }
             // clear the new frontier's flags and take its residual max / min (:484-491; max and
@@ -1061,11 +1369,23 @@ source_kernel(SourceParams<Real> p) {
                     }
                 }
                 if (__any_sync(kFullMask, item_done)) {
-                    Real s = Real(0);
+                    if constexpr (std::is_same<Real, Acc>::value) {
+                        // the eight lanes summed 0..7, then preds += xij / (ds * nr) (:386-390, :525)
+                        Real s = Real(0);
 #pragma unroll
-                    for (int b = 0; b < 8; ++b) s = radd(s, __shfl_sync(kFullMask, x, int(grp * 8 + b)));
-                    if (item_done && j == 0)
-                        p.preds[it.pos] = radd(p.preds[it.pos], rdiv(s, rmul(ds, from_u64<Real>(it.nr))));
+                        for (int b = 0; b < 8; ++b)
+                            s = radd(s, __shfl_sync(kFullMask, x, int(grp * 8 + b)));
+                        if (item_done && j == 0)
+                            p.preds[it.pos] =
+                                radd(p.preds[it.pos], rdiv(s, rmul(ds, from_u64<Real>(it.nr))));
+                    } else {
+                        double s = 0;
+#pragma unroll
+                        for (int b = 0; b < 8; ++b)
+                            s += double(__shfl_sync(kFullMask, x, int(grp * 8 + b)));
+                        if (item_done && j == 0)
+                            p.preds[it.pos] += s / (double(ds) * double(it.nr));
+                    }
                     if (item_done) has = false;
                 }
             }
@@ -1136,15 +1456,37 @@ uint64_t deadline_from_env() {
     return uint64_t(s * 1e9);
 }
 
-template <class Real>
+// FP32 weights of the mixed tau kernel for the configured omega, cached on the graph:
+// row 0 = 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) (from the same FP64 power
+// chain the parity forms use), zero at the indices the reference leaves out (0 and omega - 1).
+void prepare_mixed_tables(tgtp_graph* g, uint32_t omega) {
+    if (g->mix_omega == omega && g->mixc.ptr) return;
+    const uint32_t rows = 1 + kTauTableRows;
+    std::vector<float> t(size_t(rows) * omega, 0.f);
+    for (uint32_t i = 1; i + 1 < omega; ++i) {
+        const double lam = g->values[i];
+        const double sq = lam * lam;
+        t[i] = float(1.0 + lam);
+        double e = sq;
+        for (uint32_t k = 0; k < uint32_t(kTauTableRows); ++k) {
+            t[size_t(k + 1) * omega + i] = float(e / (1.0 - lam));
+            e *= sq;
+        }
+    }
+    g->mixc.reserve(sizeof(float) * t.size());
+    TGTP_CUDA(cudaMemcpyAsync(g->mixc.ptr, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice,
+                              g->stream));
+    TGTP_CUDA(cudaStreamSynchronize(g->stream));
+    g->mix_omega = omega;
+}
+
+// One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
+// JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
+template <class Real, class Acc, bool JACOBI, class Vec>
 void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     cudaStream_t s = g->stream;
     const uint64_t n = g->n, m = g->m;
     const uint32_t omega = uint32_t(cfg.omega);
-    const Real* vec = std::is_same<Real, float>::value ? (const Real*)g->vec_f32.ptr
-                                                        : (const Real*)g->vec_f64.ptr;
-    const Real* etab = std::is_same<Real, float>::value ? (const Real*)g->etab_f.ptr
-                                                         : (const Real*)g->etab.ptr;
     // host-side constants with the host libm (as the reference evaluates them)
     TauConst c;
     const double l1 = g->values[1], l2 = g->values[omega - 1];
@@ -1153,10 +1495,9 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     c.one_m_l2sq = 1.0 - (l2 * l2);
     c.b2 = std::log(double(1.0) / std::fabs(l2));
     const double logmd = std::log(double(m) / cfg.delta);
-    const Real eps_half = Real(cfg.epsilon / 2.0);
 
     g->taus.reserve(sizeof(int) * (m + 1));
-    g->preds.reserve(sizeof(Real) * (m + 1));
+    g->preds.reserve(sizeof(Acc) * (m + 1));
     g->stats.reserve(sizeof(unsigned long long) * kStCount);
     g->work.reserve(sizeof(unsigned) * 4);
     auto* stats = g->stats.as<unsigned long long>();
@@ -1164,7 +1505,26 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     TGTP_CUDA(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * kStCount, s));
     TGTP_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned) * 4, s));
 
-    {
+    if constexpr (JACOBI) {
+        prepare_mixed_tables(g, omega);
+        const Vec* vec = std::is_same<Vec, float>::value ? (const Vec*)g->vec_f32.ptr
+                                                          : (const Vec*)g->vec_bf16.ptr;
+        const uint64_t groups = (g->num_forward + 31) / 32;  // 32 edges per warp
+        const unsigned blocks = unsigned(std::max<uint64_t>(
+            1, std::min<uint64_t>((groups + 7) / 8, uint64_t(g->num_sms) * 8)));
+        ScopedKernel k(g->prof, s, "tau");
+        tau_mixed_kernel<Vec><<<blocks, 256, sizeof(float2) * omega, s>>>(
+            g->idx.as<uint32_t>(), g->adj.as<uint32_t>(), g->row_of.as<uint32_t>(),
+            g->rev.as<uint32_t>(), g->forward.as<uint32_t>(), g->num_forward, vec, g->omega, omega,
+            g->mixc.as<float>(), g->etab.as<double>(), g->onem.as<double>(), cfg.epsilon / 2.0,
+            double(m), c, g->taus.as<int>(), stats);
+        TGTP_LAUNCH_CHECK("tau_mixed_kernel");
+    } else {
+        const Real* vec = std::is_same<Real, float>::value ? (const Real*)g->vec_f32.ptr
+                                                            : (const Real*)g->vec_f64.ptr;
+        const Real* etab = std::is_same<Real, float>::value ? (const Real*)g->etab_f.ptr
+                                                             : (const Real*)g->etab.ptr;
+        const Real eps_half = Real(cfg.epsilon / 2.0);
         // per block: two double2 constants per index; per warp: two buffers of (x_u, x_v) chunks
         // of 32 edges x one 128-byte row piece, rows padded by one element
         const size_t tau_smem = 2 * sizeof(double2) * omega +
@@ -1190,8 +1550,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     }
 
     // source kernel.  Shared-memory tier: one warp per block, each with its residual vector and
-    // visited bitmap in shared memory (one-warp blocks give the finest occupancy steps).  Global
-    // tier (large n): 4 warps per block, vectors in HBM.  TGTP_PVEC_TIER=smem|global overrides.
+    // flags in shared memory (one-warp blocks give the finest occupancy steps).  Global tier
+    // (large n): 4 warps per block, vectors in HBM.  TGTP_PVEC_TIER=smem|global overrides.
     const size_t pv_bytes = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
     const size_t vis_bytes = (size_t(n) + 15) & ~size_t(15);
     const size_t per_warp = pv_bytes + vis_bytes + kAccBytes;
@@ -1203,7 +1563,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     const int wpb = use_smem ? 1 : 4;
     const int threads = wpb * 32;
     const size_t smem = use_smem ? per_warp * wpb : size_t(wpb) * kAccBytes;
-    auto kern = use_smem ? source_kernel<Real, true> : source_kernel<Real, false>;
+    auto kern = use_smem ? source_kernel<Real, Acc, true, JACOBI>
+                         : source_kernel<Real, Acc, false, JACOBI>;
     TGTP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
@@ -1212,30 +1573,32 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     blocks = std::min<uint64_t>(blocks, (n + wpb - 1) / wpb);
     const uint64_t warps = blocks * wpb;
     const size_t maxd = std::max<uint32_t>(g->max_degree, 1);
-    size_t scratch = warps * (2 * size_t(n) * 4 + maxd * sizeof(WalkItem));
-    if (!use_smem) scratch += warps * (size_t(n) * sizeof(Real) + size_t(n)) + 64;
-    g->scratch.reserve(scratch + 256);
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t q_bytes = align(warps * 2 * size_t(n) * 4);
+    const size_t it_bytes = align(warps * maxd * sizeof(WalkItem));
+    const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(Real)) : 0;
+    const size_t pvg_bytes = use_smem ? 0 : align(warps * size_t(n) * sizeof(Real));
+    const size_t visg_bytes = use_smem ? 0 : align(warps * vis_bytes);
+    g->scratch.reserve(q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
-    SourceParams<Real> p;
+    SourceParams<Real, Acc> p;
     p.idx = g->idx.as<uint32_t>();
     p.adj = g->adj.as<uint32_t>();
     p.deg = g->deg.as<uint32_t>();
     p.n = uint32_t(n);
     p.taus = g->taus.as<int>();
-    p.preds = g->preds.as<Real>();
+    p.preds = g->preds.as<Acc>();
     p.work = work;
     p.qbuf = reinterpret_cast<uint32_t*>(base);
-    base += warps * 2 * size_t(n) * 4;
-    base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(base) + 15) & ~uintptr_t(15));
+    base += q_bytes;
     p.items = reinterpret_cast<WalkItem*>(base);
-    base += warps * maxd * sizeof(WalkItem);
-    p.pvec_g = nullptr;
-    p.vis_g = nullptr;
-    if (!use_smem) {
-        p.pvec_g = reinterpret_cast<Real*>(base);
-        base += warps * size_t(n) * sizeof(Real);
-        p.vis_g = base;
-    }
+    base += it_bytes;
+    p.rbuf = JACOBI ? reinterpret_cast<Real*>(base) : nullptr;
+    base += rb_bytes;
+    p.pvec_g = use_smem ? nullptr : reinterpret_cast<Real*>(base);
+    base += pvg_bytes;
+    p.vis_g = use_smem ? nullptr : base;
+    p.vis_stride = vis_bytes;
     p.smem_per_warp = per_warp;
     p.max_degree = uint32_t(maxd);
     p.eps = cfg.epsilon;
@@ -1252,8 +1615,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     }
     {
         ScopedKernel k(g->prof, s, "symmetrize");
-        symmetrize_kernel<Real><<<grid_cap(m, 256, g->num_sms, 8), 256, 0, s>>>(
-            g->preds.as<Real>(), g->sym_src.as<uint32_t>(), m, out);
+        symmetrize_kernel<Acc><<<grid_cap(m, 256, g->num_sms, 8), 256, 0, s>>>(
+            g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), m, out);
         TGTP_LAUNCH_CHECK("symmetrize_kernel");
     }
 }
@@ -1278,11 +1641,22 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
     switch (cfg.precision) {
         case TGTP_PRECISION_FP32:
             if (!g->has_f32) fail(TGTP_ERR_INVALID_ARGUMENT, "FP32 form needs F32 eigenvectors");
-            run_form<float>(g, cfg, device_scores);
+            run_form<float, float, false, float>(g, cfg, device_scores);
             break;
         case TGTP_PRECISION_FP64:
             if (!g->has_f64) fail(TGTP_ERR_INVALID_ARGUMENT, "FP64 form needs F64 eigenvectors");
-            run_form<double>(g, cfg, device_scores);
+            run_form<double, double, false, double>(g, cfg, device_scores);
+            break;
+        case TGTP_PRECISION_MIXED:
+            if (cfg.vec_dtype == TGTP_VEC_BF16) {
+                if (!g->has_bf16) fail(TGTP_ERR_INVALID_ARGUMENT, "MIXED/BF16 needs BF16 eigenvectors");
+                run_form<float, double, true, __nv_bfloat16>(g, cfg, device_scores);
+            } else if (cfg.vec_dtype == TGTP_VEC_F32) {
+                if (!g->has_f32) fail(TGTP_ERR_INVALID_ARGUMENT, "MIXED/F32 needs F32 eigenvectors");
+                run_form<float, double, true, float>(g, cfg, device_scores);
+            } else {
+                fail(TGTP_ERR_INVALID_ARGUMENT, "MIXED form stores eigenvectors as F32 or BF16");
+            }
             break;
         default:
             fail(TGTP_ERR_UNSUPPORTED, "unknown precision form");

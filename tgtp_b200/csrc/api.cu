@@ -464,6 +464,7 @@ tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* 
         cudaStream_t s = g->stream;
         const uint64_t count = g->n * uint64_t(omega);
         g->omega = omega;
+        g->mix_omega = 0;
         g->values.assign(values, values + omega);
         g->d_values.reserve(sizeof(double) * omega);
         TGTP_CUDA(cudaMemcpyAsync(g->d_values.ptr, values, sizeof(double) * omega,

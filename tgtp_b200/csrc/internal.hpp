@@ -165,6 +165,8 @@ struct tgtp_graph {
     // tau-bound constants: onep[i] = 1 + lambda_i, onem[i] = 1 - lambda_i and the powers
     // lambda_i^(2(k+1)) for k < kTauTableRows, formed by the reference's repeated multiplication
     tgtp::DeviceBuffer onep, onem, etab, etab_f;
+    tgtp::DeviceBuffer mixc;     // FP32 weights of the mixed tau kernel for mix_omega
+    uint32_t mix_omega = 0;
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
