@@ -192,7 +192,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_FP32, PRECISION_FP64,
-                                VEC_F32, VEC_F64, load_eigens_txt, saba_count)
+                                PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64, load_eigens_txt,
+                                saba_count)
 
     seed = 1 + rank
     root = tempfile.mkdtemp(prefix=f"tgtp_bench_r{rank}_")
@@ -210,6 +211,7 @@ def main():
     dg.set_stream(stream.cuda_stream)
     dg.upload_eigens(values, v64, VEC_F64)
     dg.upload_eigens(values, v32, VEC_F32)
+    dg.upload_eigens(values, v32, VEC_BF16)
     out = torch.empty(m, dtype=torch.float32, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
@@ -217,8 +219,8 @@ def main():
         if world > 1:
             torch.distributed.barrier()
 
-    def timed(form: int, steps: int, warmup: int, profile: bool):
-        a = AESC(dg, AESCConfig(EPS, omega=OMEGA, gamma=GAMMA, precision=form))
+    def timed(form: int, steps: int, warmup: int, profile: bool, vec: int = VEC_F32):
+        a = AESC(dg, AESCConfig(EPS, omega=OMEGA, gamma=GAMMA, precision=form, vec_dtype=vec))
         for _ in range(warmup):
             a.tgtp_device(out.data_ptr())
         torch.cuda.synchronize()
@@ -245,7 +247,15 @@ def main():
     with ClockSampler(local) as clocks:
         ms64, wall64, k64, st64 = timed(PRECISION_FP64, args.steps, args.warmup, True)
     out64 = out.clone()
-    ms32, _, k32, st32 = timed(PRECISION_FP32, max(args.steps // 4, 10), args.warmup, True)
+    side_steps = max(args.steps // 4, 10)
+    ms32, _, k32, st32 = timed(PRECISION_FP32, side_steps, args.warmup, True)
+    mixed = {}
+    for label, vec in (("mixed_f32_vectors", VEC_F32), ("mixed_bf16_vectors", VEC_BF16)):
+        msx, _, kx, _ = timed(PRECISION_MIXED, side_steps, args.warmup, True, vec)
+        dev = (out.double() - out64.double()).abs() / out64.double().abs()
+        mixed[label] = {"ms_per_step": msx / side_steps,
+                        "kernel_ms": {k: v[1] / v[0] for k, v in kx.items()},
+                        "max_rel_dev_vs_fp64": float(dev.max())}
 
     dev_ms = torch.tensor([ms64 / args.steps], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -352,8 +362,11 @@ def main():
             "kernel_ms_sum_per_step": sum(v[1] for v in k64.values()) / args.steps,
             "clocks": clocks.summary(),
             "forms": {"fp64": {"edges_per_s": value / world, "ms_per_step": ms_step},
-                      "fp32_reference_arithmetic": {"edges_per_s": E / (ms32 / max(args.steps // 4, 10) * 1e-3),
-                                                    "kernel_ms": {k: v[1] / v[0] for k, v in k32.items()}}},
+                      "fp32_reference_arithmetic": {"edges_per_s": E / (ms32 / side_steps * 1e-3),
+                                                    "kernel_ms": {k: v[1] / v[0] for k, v in k32.items()}},
+                      **{k: dict(v, edges_per_s=E / (v["ms_per_step"] * 1e-3),
+                                 speedup_vs_fp64=ms_step / v["ms_per_step"])
+                         for k, v in mixed.items()}},
             "saba": saba,
             "wall_s_timed_region": wall64,
         }
