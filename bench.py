@@ -297,14 +297,20 @@ def main():
     line = None
     if rank == 0:
         hbm, peak_kind = peaks()
-        # dominant kernel of the FP64 form and its algorithmic bytes (tau: 2 omega 8-byte reads
-        # per undirected edge; source: 20 B per push traversal + 12 B per frontier vertex +
-        # 32 B per 2-walker hop; symmetrise: 12 B per slot)
+        # algorithmic bytes per launch of each kernel of the FP64 form:
+        #   tau_sums: both omega-element FP64 eigen rows of every undirected edge, its 16-byte record
+        #             and the 16-byte (upsilon, delta_0) sums written;
+        #   tau_bound: record, sums, two degrees and two tau words per edge, plus both rows again for
+        #             every further delta sweep (tau_iterations - E of them);
+        #   source: 20 B per push traversal + 12 B per frontier vertex + 32 B per 2-walker hop;
+        #   finish: 24 B per slot
+        E_fwd = E
         per_launch = {
-            "tau": 2 * OMEGA * 8 * E,
+            "tau_sums": E_fwd * (2 * OMEGA * 8 + 32),
+            "tau_bound": E_fwd * 48 + 2 * OMEGA * 8 * max(st64["tau_iterations"] - E_fwd, 0),
             "source": 20 * st64["push_traversals"] + 12 * st64["push_vertices"]
                       + 32 * st64["walk_hops"],
-            "symmetrize": 12 * m,
+            "finish": 24 * m,
         }
         top = max(k64, key=lambda k: k64[k][1])
         launches, tot = k64[top]

@@ -163,6 +163,7 @@ DEFINE_KTH(double, kth_largest_f64)
 #define REAL double
 #define VEC double
 #define FN(name) CAT(name, _f64)
+#define SPLIT_SUMS 1
 #include "tgtp_oracle_body.inc"
 #undef REAL
 #undef VEC

@@ -50,6 +50,20 @@ enum StatIdx {
     kStWalkHops, kStFallback, kStTauIters, kStTauAmbiguous, kStPhase0,
     kStCount = kStPhase0 + 8
 };
+// The run counters are striped over kStStripes copies (block index modulo kStStripes) so that the
+// warps of a launch do not all meet on one address; the host adds the copies up.
+constexpr int kStStripes = 32;
+
+// The run's work words ([0] next list entry, [1] error flags, [2] list length) sit behind the
+// striped counters in the same buffer.
+inline unsigned* run_work(tgtp_graph* g) {
+    return reinterpret_cast<unsigned*>(g->stats.as<unsigned char>() +
+                                       sizeof(unsigned long long) * kStCount * kStStripes);
+}
+
+__device__ __forceinline__ void stat_add(unsigned long long* stats, int i, unsigned long long v) {
+    if (v) atomicAdd(stats + size_t(blockIdx.x % kStStripes) * kStCount + i, v);
+}
 
 struct TauConst {
     double one_m_l1sq, b1;  // 1 - lambda_1^2, log(1/|lambda_1|)
@@ -93,6 +107,23 @@ __device__ __forceinline__ Real etab_value(const Real* tab, const double* tabd, 
     const double sq = __ldg(tabd + i);
     for (uint32_t r = kTauTableRows - 1; r < k; ++r) e = __dmul_rn(e, sq);
     return from_f64<Real>(e);
+}
+
+// Rows whose every tau is at most 1 stop after their first push round: with ell = 1 every slot has
+// rest = tau - ell <= 0, so rwcost = 0 <= picost (src/aesc.h:483-502) and no slot walks
+// (:508-526).  Their scores follow from the closed-form first round and they skip the source
+// kernel.  The tau kernels mark each row that has a slot with tau > 1 (mark[r] == epoch) and append
+// it, once per run, to the list the source kernel claims its sources from.
+struct RowMarks {
+    uint32_t* mark;
+    uint32_t* list;
+    unsigned* len;
+    uint32_t epoch;
+};
+
+__device__ __forceinline__ void mark_row(const RowMarks& rm, uint32_t r) {
+    if (*reinterpret_cast<volatile const uint32_t*>(rm.mark + r) == rm.epoch) return;
+    if (atomicExch(rm.mark + r, rm.epoch) != rm.epoch) rm.list[atomicAdd(rm.len, 1u)] = r;
 }
 
 // ---- stage 1: tau per undirected edge ------------------------------------------------------------
@@ -141,7 +172,8 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
            const Real* __restrict__ vec, uint32_t stride, uint32_t omega,
            const double* __restrict__ onep_g, const double* __restrict__ onem_g,
            const Real* __restrict__ etab, const double* __restrict__ etabd, Real epsilon,
-           uint64_t m, TauConst c, int* __restrict__ taus, unsigned long long* __restrict__ stats) {
+           uint64_t m, TauConst c, int* __restrict__ taus, RowMarks rm,
+           unsigned long long* __restrict__ stats) {
     constexpr uint32_t CH = 128 / sizeof(Real);  // chunk: one 128-byte row piece
     constexpr uint32_t LD = CH + 1;              // odd tile stride: conflict-free own-row reads
     extern __shared__ __align__(16) unsigned char tsm[];
@@ -259,6 +291,10 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
                     done = true;
                     taus[pos] = tau;
                     taus[__ldg(rev + pos)] = tau;
+                    if (tau > 1) {
+                        mark_row(rm, u);
+                        mark_row(rm, v);
+                    }
                 }
             }
         }
@@ -269,8 +305,8 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
         ambiguous += __shfl_xor_sync(kFullMask, ambiguous, o);
     }
     if (lane == 0) {
-        if (iters) atomicAdd(stats + kStTauIters, iters);
-        if (ambiguous) atomicAdd(stats + kStTauAmbiguous, ambiguous);
+        stat_add(stats, kStTauIters, iters);
+        stat_add(stats, kStTauAmbiguous, ambiguous);
     }
 }
 
@@ -303,20 +339,6 @@ __device__ __forceinline__ int get_tau_mixed(double inv1, double inv2, double ep
     return tau % 2 == 0 ? tau + 1 : tau;
 }
 
-// Weight of index i in delta_k (mixed form): lambda_i^(2(k+1)) / (1 - lambda_i) in FP32, zero at the
-// indices the reference leaves out; beyond the precomputed rows the FP64 power chain continues.
-__device__ __forceinline__ float mixed_weight(const float* __restrict__ mixc,
-                                              const double* __restrict__ etabd,
-                                              const double* __restrict__ onem, uint32_t stride,
-                                              uint32_t omega, uint32_t k, uint32_t i) {
-    if (i < 1 || i + 1 >= omega) return 0.f;
-    if (k < uint32_t(kTauTableRows)) return __ldg(mixc + size_t(k + 1) * omega + i);
-    double ev = __ldg(etabd + size_t(kTauTableRows - 1) * stride + i);
-    const double sq = __ldg(etabd + i);
-    for (uint32_t r = kTauTableRows - 1; r < k; ++r) ev *= sq;
-    return float(ev / __ldg(onem + i));
-}
-
 // Error-free combination of the eight partial sums of a lane group (TwoSum tree, the rounding
 // errors carried and added back).
 __device__ __forceinline__ double group_reduce(float a) {
@@ -333,113 +355,281 @@ __device__ __forceinline__ double group_reduce(float a) {
     return double(a) + double(ca);
 }
 
-// The mixed tau kernel.  A warp works on 32 forward slots at a time, four at once: the 8 lanes of
-// group g take slot 4 s + g at step s and hold indices i = l, l + 8, ... of its two eigen rows
-// (32-byte row pieces per group).  Each lane accumulates its terms d_i^2 w_i with FMAs (the terms are
-// non-negative, so a lane's sum has relative error below 16 ulp); the group's eight partial sums
-// are combined by group_reduce.  The slot's sums land in lane 4 s + g, and every lane then
-// evaluates its own slot's bound in FP64 at once.
+// ---- stage 1 (FP64 and mixed forms): tau with eight lanes per edge ---------------------------------
+// A warp takes four forward slots at a time, one per group of eight lanes.  Lane s of a group owns
+// the index pieces {C j + P s, ..., C j + P s + P - 1} of the slot's two eigen rows (P = 2 FP64,
+// 4 F32, 8 BF16 elements: one 16-byte load per row and piece; C = 8 P) and accumulates the terms
+// d_i^2 w_i over them with fused multiply-adds, in index order, where d_i = x_u[i] - x_v[i] and
+// w_i = 1 + lambda_i (upsilon, src/aesc.h:151-162) or lambda_i^(2(k+1)) / (1 - lambda_i) (delta_k,
+// :137-150).  The weights are exactly zero at the indices the reference leaves out (0 and
+// omega - 1) and past omega, so those terms add nothing.  The eight partial sums are combined by a
+// fixed tree: ((S0 + S1) + (S2 + S3)) + ((S4 + S5) + (S6 + S7)) in FP64 for the FP64 form, the
+// compensated group_reduce into FP64 for the mixed form.  The bound and the delta iteration follow
+// :164-216 (get_tau, t += 2 while t <= tau' < tau).
+template <class Vec> struct Split;
+template <> struct Split<double> {
+    static constexpr uint32_t P = 2;
+    using Part = double;
+};
+template <> struct Split<float> {
+    static constexpr uint32_t P = 4;
+    using Part = float;
+};
+template <> struct Split<__nv_bfloat16> {
+    static constexpr uint32_t P = 8;
+    using Part = float;
+};
+
+// P consecutive elements starting at i0 (a multiple of P below omega); one 16-byte load when the
+// row stride keeps pieces aligned, else element loads masked at omega.
+__device__ __forceinline__ void load_piece(const double* __restrict__ row, uint32_t i0,
+                                           uint32_t omega, bool vec_ok, double (&x)[2]) {
+    if (vec_ok) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(row + i0));
+        x[0] = t.x;
+        x[1] = t.y;
+    } else {
+        x[0] = __ldg(row + i0);
+        x[1] = i0 + 1 < omega ? __ldg(row + i0 + 1) : 0.0;
+    }
+}
+__device__ __forceinline__ void load_piece(const float* __restrict__ row, uint32_t i0,
+                                           uint32_t omega, bool vec_ok, float (&x)[4]) {
+    if (vec_ok) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(row + i0));
+        x[0] = t.x;
+        x[1] = t.y;
+        x[2] = t.z;
+        x[3] = t.w;
+    } else {
+#pragma unroll
+        for (uint32_t e = 0; e < 4; ++e) x[e] = i0 + e < omega ? __ldg(row + i0 + e) : 0.f;
+    }
+}
+__device__ __forceinline__ void load_piece(const __nv_bfloat16* __restrict__ row, uint32_t i0,
+                                           uint32_t omega, bool vec_ok, float (&x)[8]) {
+    if (vec_ok) {
+        const uint4 t = __ldg(reinterpret_cast<const uint4*>(row + i0));
+        const uint32_t w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {  // a bf16 is the upper half of its float
+            x[2 * h] = __uint_as_float(w[h] << 16);
+            x[2 * h + 1] = __uint_as_float(w[h] & 0xffff0000u);
+        }
+    } else {
+#pragma unroll
+        for (uint32_t e = 0; e < 8; ++e) x[e] = i0 + e < omega ? vec_load(row + i0 + e) : 0.f;
+    }
+}
+
+__device__ __forceinline__ double split_fma(double a, double w, double s) {
+    const double d2 = __dmul_rn(a, a);
+    return __fma_rn(d2, w, s);
+}
+__device__ __forceinline__ float split_fma(float a, float w, float s) {
+    const float d2 = __fmul_rn(a, a);
+    return __fmaf_rn(d2, w, s);
+}
+__device__ __forceinline__ double split_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float split_sub(float a, float b) { return __fsub_rn(a, b); }
+
+__device__ __forceinline__ double split_reduce(double s) {
+    s = __dadd_rn(s, __shfl_xor_sync(kFullMask, s, 1));
+    s = __dadd_rn(s, __shfl_xor_sync(kFullMask, s, 2));
+    return __dadd_rn(s, __shfl_xor_sync(kFullMask, s, 4));
+}
+__device__ __forceinline__ double split_reduce(float s) { return group_reduce(s); }
+
+// Weight of index i in delta_k: row k + 1 of the padded table while k < kTauTableRows, beyond it
+// the FP64 power chain continued from the last row of the eigen_t_1 table (src/aesc.h:201-203).
+template <class Part>
+__device__ __forceinline__ Part split_weight(const Part* __restrict__ wtab, uint32_t wpad,
+                                             uint32_t k, uint32_t i, uint32_t omega,
+                                             const double* __restrict__ etabd, uint32_t stride,
+                                             const double* __restrict__ onem) {
+    if (k < uint32_t(kTauTableRows)) return __ldg(wtab + size_t(k + 1) * wpad + i);
+    if (i < 1 || i + 1 >= omega) return Part(0);
+    double e = __ldg(etabd + size_t(kTauTableRows - 1) * stride + i);
+    const double sq = __ldg(etabd + i);
+    for (uint32_t r = kTauTableRows - 1; r < k; ++r) e = __dmul_rn(e, sq);
+    return Part(__ddiv_rn(e, __ldg(onem + i)));
+}
+
+// Pass of one 8-lane group over the rows of one edge: lane sl's partial sums of d_i^2 wa_i and
+// d_i^2 wb_i (two weight rows at once) or of d_i^2 w(k, i) alone.
+template <class Vec, int ROWS>
+__device__ __forceinline__ void split_pass(const Vec* __restrict__ ur, const Vec* __restrict__ vr,
+                                           uint32_t omega, bool vec_ok, uint32_t sl,
+                                           const typename Split<Vec>::Part* wa,
+                                           const typename Split<Vec>::Part* wb,
+                                           typename Split<Vec>::Part& sa,
+                                           typename Split<Vec>::Part& sb) {
+    using Part = typename Split<Vec>::Part;
+    constexpr uint32_t P = Split<Vec>::P, C = 8 * P;
+#pragma unroll 4
+    for (uint32_t i0 = sl * P; i0 < omega; i0 += C) {
+        Part xu[P], xv[P];
+        load_piece(ur, i0, omega, vec_ok, xu);
+        load_piece(vr, i0, omega, vec_ok, xv);
+#pragma unroll
+        for (uint32_t j = 0; j < P; ++j) {
+            const Part d = split_sub(xu[j], xv[j]);
+            if (ROWS == 2) sa = split_fma(d, wa[i0 + j], sa);
+            sb = split_fma(d, wb[i0 + j], sb);
+        }
+    }
+}
+
+// Stage 1a: the first sweep of every forward edge (upsilon and delta_0 sums), a pure gather.  A
+// warp takes eight edges at a time, two per group; the edge records of the next step are fetched
+// one step ahead.
 template <class Vec>
-__global__ void __launch_bounds__(256)
-tau_mixed_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
-                 const uint32_t* __restrict__ row_of, const uint32_t* __restrict__ rev,
-                 const uint32_t* __restrict__ forward, uint64_t num_forward,
-                 const Vec* __restrict__ vec, uint32_t stride, uint32_t omega,
-                 const float* __restrict__ mixc, const double* __restrict__ etabd,
-                 const double* __restrict__ onem, double eps_half, double mdbl, TauConst c,
-                 int* __restrict__ taus, unsigned long long* __restrict__ stats) {
-    extern __shared__ __align__(16) unsigned char msm[];
-    float2* w01 = reinterpret_cast<float2*>(msm);  // (1 + lambda_i, delta_0 weight of index i)
-    for (uint32_t i = threadIdx.x; i < omega; i += blockDim.x)
-        w01[i] = make_float2(__ldg(mixc + i), __ldg(mixc + omega + i));
+__global__ void __launch_bounds__(256, 4)
+tau_sums_kernel(const uint4* __restrict__ fedge, uint64_t num_forward, const Vec* __restrict__ vec,
+                uint32_t stride, uint32_t omega, const typename Split<Vec>::Part* __restrict__ wtab,
+                uint32_t wpad, double2* __restrict__ sums) {
+    using Part = typename Split<Vec>::Part;
+    extern __shared__ __align__(16) unsigned char ssm[];
+    Part* wu = reinterpret_cast<Part*>(ssm);  // upsilon weights, then delta_0 weights
+    Part* wd = wu + wpad;
+    for (uint32_t i = threadIdx.x; i < 2 * wpad; i += blockDim.x) wu[i] = __ldg(wtab + i);
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31, grp = lane >> 3, sl = lane & 7;
     const uint64_t gw = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const bool vec_ok = stride % Split<Vec>::P == 0;
+    uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+    if (gw * 8 + grp < num_forward) n0 = __ldg(fedge + gw * 8 + grp);
+    if (gw * 8 + 4 + grp < num_forward) n1 = __ldg(fedge + gw * 8 + 4 + grp);
+    for (uint64_t base = gw * 8; base < num_forward; base += nw * 8) {
+        const uint64_t e0 = base + grp, e1 = e0 + 4;
+        const uint4 r0 = n0, r1 = n1;
+        if (e0 + nw * 8 < num_forward) n0 = __ldg(fedge + e0 + nw * 8);
+        if (e1 + nw * 8 < num_forward) n1 = __ldg(fedge + e1 + nw * 8);
+        Part su0 = Part(0), sd0 = Part(0), su1 = Part(0), sd1 = Part(0);
+        if (e0 < num_forward)
+            split_pass<Vec, 2>(vec + size_t(r0.x) * stride, vec + size_t(r0.y) * stride, omega,
+                               vec_ok, sl, wu, wd, su0, sd0);
+        if (e1 < num_forward)
+            split_pass<Vec, 2>(vec + size_t(r1.x) * stride, vec + size_t(r1.y) * stride, omega,
+                               vec_ok, sl, wu, wd, su1, sd1);
+        const double u0 = split_reduce(su0), d0 = split_reduce(sd0);
+        const double u1 = split_reduce(su1), d1 = split_reduce(sd1);
+        if (sl == 0 && e0 < num_forward) sums[e0] = make_double2(u0, d0);
+        if (sl == 0 && e1 < num_forward) sums[e1] = make_double2(u1, d1);
+    }
+}
+
+// Stage 1b: the bound per edge, one lane per edge (src/aesc.h:181-207): tau_0 from lambda_1, then
+// tau' from delta_k while t <= tau' < tau (t += 2).  Edges that need a further delta sweep are
+// served four at a time by the warp's 8-lane groups.  Writes tau to both slots and marks the two
+// rows when tau > 1.
+template <class Vec>
+__global__ void __launch_bounds__(256)
+tau_bound_kernel(const uint4* __restrict__ fedge, const uint32_t* __restrict__ deg,
+                 uint64_t num_forward, const double2* __restrict__ sums,
+                 const Vec* __restrict__ vec, uint32_t stride, uint32_t omega,
+                 const typename Split<Vec>::Part* __restrict__ wtab, uint32_t wpad,
+                 const double* __restrict__ etabd, const double* __restrict__ onem,
+                 double eps_half, uint64_t m, TauConst c, int* __restrict__ taus, RowMarks rm,
+                 unsigned long long* __restrict__ stats) {
+    using Part = typename Split<Vec>::Part;
+    constexpr bool kF64 = std::is_same<Vec, double>::value;
+    constexpr uint32_t P = Split<Vec>::P, C = 8 * P;
+    const uint32_t lane = threadIdx.x & 31, grp = lane >> 3, sl = lane & 7;
+    const uint64_t gw = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const bool vec_ok = stride % P == 0;
+    const double mdbl = double(m);
     const double inv_b1 = 1.0 / c.b1, inv_b2 = 1.0 / c.b2;
-    unsigned long long iters = 0;
+    unsigned long long iters = 0, ambiguous = 0;
     for (uint64_t base = gw * 32; base < num_forward; base += nw * 32) {
         const uint64_t e = base + lane;
         const bool act = e < num_forward;
-        uint32_t pos = 0, u = 0, v = 0, du = 1, dv = 1;
+        uint4 rec = make_uint4(0, 0, 0, 0);
+        double2 sm = make_double2(0.0, 0.0);
+        uint32_t du = 1, dv = 1;
         if (act) {
-            pos = __ldg(forward + e);
-            u = __ldg(row_of + pos);
-            v = __ldg(adj + pos);
-            du = __ldg(idx + u + 1) - __ldg(idx + u);
-            dv = __ldg(idx + v + 1) - __ldg(idx + v);
-        }
-        double ups = 0, del = 0;
-        for (uint32_t st = 0; st < 8; ++st) {
-            const uint32_t t = st * 4 + grp;
-            const Vec* ur = vec + size_t(__shfl_sync(kFullMask, u, t)) * stride;
-            const Vec* vr = vec + size_t(__shfl_sync(kFullMask, v, t)) * stride;
-            float a = 0.f, b = 0.f;
-#pragma unroll 4
-            for (uint32_t i = sl; i < omega; i += 8) {
-                const float d = vec_load(ur + i) - vec_load(vr + i);
-                const float d2 = d * d;
-                const float2 wi = w01[i];
-                a = __fmaf_rn(d2, wi.x, a);
-                b = __fmaf_rn(d2, wi.y, b);
-            }
-            const double s1 = group_reduce(a), s2 = group_reduce(b);
-            const uint32_t from = (lane & 3) * 8;  // lane 4 st + g takes group g's sums
-            const double r1 = __shfl_sync(kFullMask, s1, from);
-            const double r2 = __shfl_sync(kFullMask, s2, from);
-            if ((lane >> 2) == st) {
-                ups = r1 / mdbl;
-                del = r2 / mdbl;
-            }
+            rec = __ldg(fedge + e);
+            sm = sums[e];
+            du = __ldg(deg + rec.x);
+            dv = __ldg(deg + rec.y);
         }
         const double inv1 = 1.0 / double(du), inv2 = 1.0 / double(dv);
-        int tau = 0, tsteps = 1;
-        uint32_t k = 0;
+        auto bound = [&](double one_m_lam2, double b, double inv_b, double dl, double up) {
+            if constexpr (kF64) {
+                return get_tau<double>(du, dv, eps_half, one_m_lam2, b, dl, up, ambiguous);
+            } else {
+                return get_tau_mixed(inv1, inv2, eps_half, one_m_lam2, inv_b, dl, up);
+            }
+        };
+        int tau = 0, t = 1;
+        uint32_t k = 1;
         bool need = false;
+        double ups = 0;
         if (act) {
-            tau = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l1sq, inv_b1, 0.0, 0.0);
+            ups = kF64 ? __ddiv_rn(sm.x, mdbl) : sm.x / mdbl;
+            const double del = kF64 ? __ddiv_rn(sm.y, mdbl) : sm.y / mdbl;
+            tau = bound(c.one_m_l1sq, c.b1, inv_b1, 0.0, 0.0);
             ++iters;
-            const int tp = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l2sq, inv_b2, del, ups);
-            if (tsteps <= tp && tp < tau) {
+            const int tp = bound(c.one_m_l2sq, c.b2, inv_b2, del, ups);
+            if (t <= tp && tp < tau) {
                 tau = tp;
-                tsteps += 2;
-                k = 1;
+                t += 2;
                 need = true;
             }
         }
-        // further delta iterations (:191-204) for slots that still improve, four at a time
-        while (true) {
-            unsigned nb = __ballot_sync(kFullMask, need);
-            if (!nb) break;
-            while (nb) {
-                int sel[4];
+        // further delta sweeps (:191-204), four edges at a time
+        unsigned nb;
+        while ((nb = __ballot_sync(kFullMask, need)) != 0) {
+            int sel[4];
 #pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    sel[g] = nb ? __ffs(nb) - 1 : -1;
-                    if (nb) nb &= nb - 1;
-                }
-                const uint32_t tt = sel[grp] < 0 ? 0u : uint32_t(sel[grp]);
-                const Vec* ur = vec + size_t(__shfl_sync(kFullMask, u, tt)) * stride;
-                const Vec* vr = vec + size_t(__shfl_sync(kFullMask, v, tt)) * stride;
-                const uint32_t kt = __shfl_sync(kFullMask, k, tt);
-                float b = 0.f;
-                for (uint32_t i = sl; i < omega; i += 8) {
-                    const float d = vec_load(ur + i) - vec_load(vr + i);
-                    b = __fmaf_rn(d * d, mixed_weight(mixc, etabd, onem, stride, omega, kt, i), b);
-                }
-                const double dk = group_reduce(b);
+            for (int g = 0; g < 4; ++g) {
+                sel[g] = nb ? __ffs(nb) - 1 : -1;
+                if (nb) nb &= nb - 1;
+            }
+            const uint32_t src_lane = sel[grp] < 0 ? 0u : uint32_t(sel[grp]);
+            const uint32_t gu = __shfl_sync(kFullMask, rec.x, src_lane);
+            const uint32_t gv = __shfl_sync(kFullMask, rec.y, src_lane);
+            const uint32_t gk = __shfl_sync(kFullMask, k, src_lane);
+            Part s2 = Part(0);
+            if (sel[grp] >= 0) {
+                const Vec* ur = vec + size_t(gu) * stride;
+                const Vec* vr = vec + size_t(gv) * stride;
+                if (gk < uint32_t(kTauTableRows)) {
+                    split_pass<Vec, 1>(ur, vr, omega, vec_ok, sl, nullptr,
+                                       wtab + size_t(gk + 1) * wpad, s2, s2);
+                } else {
+                    for (uint32_t i0 = sl * P; i0 < omega; i0 += C) {
+                        Part xu[P], xv[P];
+                        load_piece(ur, i0, omega, vec_ok, xu);
+                        load_piece(vr, i0, omega, vec_ok, xv);
 #pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    const double r = __shfl_sync(kFullMask, dk, g * 8);
-                    if (sel[g] >= 0 && lane == uint32_t(sel[g])) del = r / mdbl;
+                        for (uint32_t j = 0; j < P; ++j)
+                            s2 = split_fma(split_sub(xu[j], xv[j]),
+                                           split_weight<Part>(wtab, wpad, gk, i0 + j, omega, etabd,
+                                                              stride, onem),
+                                           s2);
+                    }
                 }
             }
-            if (need) {
+            const double dsum = split_reduce(s2);
+            double mine = 0.0;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                const double r = __shfl_sync(kFullMask, dsum, g * 8);
+                if (sel[g] == int(lane)) mine = r;
+            }
+            bool served = false;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) served |= sel[g] == int(lane);
+            if (served) {
+                const double del = kF64 ? __ddiv_rn(mine, mdbl) : mine / mdbl;
                 ++iters;
-                const int tp = get_tau_mixed(inv1, inv2, eps_half, c.one_m_l2sq, inv_b2, del, ups);
-                if (tsteps <= tp && tp < tau) {
+                const int tp = bound(c.one_m_l2sq, c.b2, inv_b2, del, ups);
+                if (t <= tp && tp < tau) {
                     tau = tp;
-                    tsteps += 2;
+                    t += 2;
                     ++k;
                 } else {
                     need = false;
@@ -447,13 +637,23 @@ tau_mixed_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ 
             }
         }
         if (act) {
-            taus[pos] = tau;
-            taus[__ldg(rev + pos)] = tau;
+            taus[rec.z] = tau;
+            taus[rec.w] = tau;
+            if (tau > 1) {
+                mark_row(rm, rec.x);
+                mark_row(rm, rec.y);
+            }
         }
     }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) iters += __shfl_xor_sync(kFullMask, iters, o);
-    if (lane == 0 && iters) atomicAdd(stats + kStTauIters, iters);
+    for (int o = 16; o; o >>= 1) {
+        iters += __shfl_xor_sync(kFullMask, iters, o);
+        ambiguous += __shfl_xor_sync(kFullMask, ambiguous, o);
+    }
+    if (lane == 0) {
+        stat_add(stats, kStTauIters, iters);
+        stat_add(stats, kStTauAmbiguous, ambiguous);
+    }
 }
 
 // ---- stage 2: per-source push, edge bound and walks -----------------------------------------------
@@ -470,7 +670,8 @@ struct SourceParams {
     uint32_t n;
     const int* taus;
     Acc* preds;           // pre-symmetric row scores (Real in the parity forms, double in MIXED)
-    unsigned* work;       // [0] next source, [1] error flags
+    unsigned* work;       // [0] next list entry, [1] error flags, [2] list length
+    const uint32_t* rows; // the sources to run (rows with a slot of tau > 1), in any order
     uint32_t* qbuf;       // 2 * n per warp
     WalkItem* items;      // max_degree per warp
     Real* pvec_g;         // n per warp (global tier)
@@ -482,7 +683,6 @@ struct SourceParams {
     double eps;
     double logmd;         // log(m / delta), formed on the host
     int gamma;
-    int* ell_out;
     unsigned long long* stats;
     const uint2* adjd;    // (neighbour, neighbour degree) per slot
     uint64_t budget_ns;   // device time budget; past it every warp stops and flags a timeout
@@ -673,10 +873,7 @@ source_kernel(SourceParams<Real, Acc> p) {
         vis = p.vis_g + gw * p.vis_stride;
         acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
-    for (uint32_t i = lane; i < n; i += 32) {
-        pvec[i] = Real(0);
-        vis[i] = 0;
-    }
+    bool cleared = false;  // pvec and flags are zeroed once, before the warp's first source
     uint32_t* qa = p.qbuf + gw * 2 * size_t(n);
     uint32_t* qb = qa + n;
     WalkItem* items = p.items + gw * size_t(p.max_degree);
@@ -697,16 +894,33 @@ source_kernel(SourceParams<Real, Acc> p) {
     };
     __syncwarp();
 
+    const unsigned nrows = p.work[2];  // final: the tau kernel that appends to the list has ended
+    // list entry gw first, then entries past the grid's warps claimed one at a time (warps past
+    // the list's end leave without touching the counter)
+    const uint64_t nwarps = uint64_t(gridDim.x) * wpb;
+    bool first_claim = true;
     while (true) {
-        unsigned k = 0;
-        if (lane == 0) k = atomicAdd(p.work, 1u);
-        k = __shfl_sync(kFullMask, k, 0);
-        if (k >= n) break;
+        uint64_t k = gw;
+        if (!first_claim) {
+            unsigned c = 0;
+            if (lane == 0) c = atomicAdd(p.work, 1u);
+            k = nwarps + __shfl_sync(kFullMask, c, 0);
+        }
+        first_claim = false;
+        if (k >= nrows) break;
         if (globaltimer_ns() > deadline) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);
             break;
         }
-        const uint32_t src = k;
+        const uint32_t src = __ldg(p.rows + k);
+        if (!cleared) {
+            for (uint32_t i = lane; i < n; i += 32) {
+                pvec[i] = Real(0);
+                vis[i] = 0;
+            }
+            cleared = true;
+            __syncwarp();
+        }
         uint32_t* q = qa;
         uint32_t* qn = qb;
         const uint32_t rb = __ldg(idx + src), re = __ldg(idx + src + 1);
@@ -1070,7 +1284,6 @@ source_kernel(SourceParams<Real, Acc> p) {
             break;
         }
         st_rounds += ell;
-        if (lane == 0 && p.ell_out) p.ell_out[src] = ell;
 
         // slots that still need walks (rest = tau - ell > 0), compacted in slot order
         uint32_t nitems = 0;
@@ -1411,34 +1624,73 @@ source_kernel(SourceParams<Real, Acc> p) {
         lap(7);
     }
     if (lane == 0) {
-        atomicAdd(p.stats + kStPushRounds, st_rounds);
-        atomicAdd(p.stats + kStPushVertices, st_pv);
-        atomicAdd(p.stats + kStPushTraversals, st_tr);
+        stat_add(p.stats, kStPushRounds, st_rounds);
+        stat_add(p.stats, kStPushVertices, st_pv);
+        stat_add(p.stats, kStPushTraversals, st_tr);
     }
     st_we = warp_sum_u64(st_we);
     st_wc = warp_sum_u64(st_wc);
     st_wh = warp_sum_u64(st_wh);
     st_fb = warp_sum_u64(st_fb);
     if (lane == 0) {
-        atomicAdd(p.stats + kStWalkEdges, st_we);
-        atomicAdd(p.stats + kStWalkCount, st_wc);
-        atomicAdd(p.stats + kStWalkHops, st_wh);
-        atomicAdd(p.stats + kStFallback, st_fb);
+        stat_add(p.stats, kStWalkEdges, st_we);
+        stat_add(p.stats, kStWalkCount, st_wc);
+        stat_add(p.stats, kStWalkHops, st_wh);
+        stat_add(p.stats, kStFallback, st_fb);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) atomicAdd(p.stats + kStPhase0 + i, (unsigned long long)ph[i]);
+        for (int i = 0; i < 8; ++i) stat_add(p.stats, kStPhase0 + i, (unsigned long long)ph[i]);
     }
 }
 
-// ---- stage 3: symmetrise -------------------------------------------------------------------------
-template <class Real>
-__global__ void symmetrize_kernel(const Real* __restrict__ preds, const uint32_t* __restrict__ sym_src,
-                                  uint64_t m, float* __restrict__ out) {
+// ---- stage 3: symmetrise (src/aesc.h:532-550) -----------------------------------------------------
+// score[q] = p[q] + p[q'] with q' the slot that lands on q (sym_src; none in a row without its
+// reverse).  p comes from the source kernel for listed rows, and in closed form for the others:
+// after the first round of source s, pvec[s] = 0 and pvec[u] = 1 / deg(u) for each neighbour u, so
+// p[s -> u] = 1 / ds + (0 - 1 / deg(u)) / ds in the form's arithmetic.  Those rows' work counters
+// (one round, one frontier vertex, ds traversals) are added here.
+template <class Real, class Acc>
+__device__ __forceinline__ Acc closed_row_score(uint32_t ds, uint32_t du) {
+    const Real d = from_u64<Real>(ds);
+    const Acc pinit = from_f64<Acc>(__ddiv_rn(1.0, double(d)));
+    return row_update<Real, Acc>(pinit, Real(0), rdiv(Real(1), from_u64<Real>(du)), d);
+}
+
+template <class Real, class Acc>
+__global__ void __launch_bounds__(256)
+finish_kernel(const Acc* __restrict__ preds, const uint32_t* __restrict__ sym_src,
+              const uint32_t* __restrict__ row_of, const uint2* __restrict__ adjd,
+              const uint32_t* __restrict__ deg, const uint32_t* __restrict__ mark, uint32_t epoch,
+              uint64_t m, float* __restrict__ out, unsigned long long* __restrict__ stats) {
+    unsigned long long rows = 0, trav = 0;
     for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < m;
          q += uint64_t(gridDim.x) * blockDim.x) {
-        Real s = preds[q];
-        const uint32_t o = sym_src[q];
-        if (o) s = radd(s, preds[o - 1]);
-        out[q] = float(s);
+        // first level: the slot's row, its (neighbour, degree) and the slot landing on it
+        const uint32_t s = __ldg(row_of + q);
+        const uint2 tv = __ldg(adjd + q);
+        const uint32_t o = __ldg(sym_src + q);
+        const bool first = q == 0 || __ldg(row_of + q - 1) != s;
+        // second level, all at once: both rows' marks, both pre-symmetric scores, and the degree of
+        // s (the reverse slot's neighbour degree; tgtp_run takes no repeated neighbours)
+        const uint32_t r = o ? o - 1 : 0;
+        const bool ls = __ldg(mark + s) == epoch;
+        const bool lt = o && __ldg(mark + tv.x) == epoch;  // slot r lies in row tv.x
+        const Acc pq = preds[q];
+        const Acc pr = o ? preds[r] : Acc(0);
+        const uint32_t ds = o ? __ldg(adjd + r).y : __ldg(deg + s);
+        Acc a = ls ? pq : closed_row_score<Real, Acc>(ds, tv.y);
+        if (!ls && first) {
+            ++rows;
+            trav += ds;
+        }
+        if (o) a = radd(a, lt ? pr : closed_row_score<Real, Acc>(tv.y, ds));
+        out[q] = float(a);
+    }
+    rows = warp_sum_u64(rows);
+    trav = warp_sum_u64(trav);
+    if ((threadIdx.x & 31) == 0) {
+        stat_add(stats, kStPushRounds, rows);
+        stat_add(stats, kStPushVertices, rows);
+        stat_add(stats, kStPushTraversals, trav);
     }
 }
 
@@ -1456,28 +1708,59 @@ uint64_t deadline_from_env() {
     return uint64_t(s * 1e9);
 }
 
-// FP32 weights of the mixed tau kernel for the configured omega, cached on the graph:
-// row 0 = 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) (from the same FP64 power
-// chain the parity forms use), zero at the indices the reference leaves out (0 and omega - 1).
-void prepare_mixed_tables(tgtp_graph* g, uint32_t omega) {
-    if (g->mix_omega == omega && g->mixc.ptr) return;
-    const uint32_t rows = 1 + kTauTableRows;
-    std::vector<float> t(size_t(rows) * omega, 0.f);
+// Weight tables of the split tau kernel for the configured omega, cached on the graph: row 0 =
+// 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) from the same FP64 power chain as the
+// parity forms' eigen_t_1 table, zero at the indices the reference leaves out (0 and omega - 1)
+// and in the padding of each row to a multiple of 64.  FP64 for the FP64 form, FP32 (rounded from
+// the FP64 values) for the mixed form.
+uint32_t split_pad(uint32_t omega) { return (omega + 63u) & ~63u; }
+
+void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
+    if (g->split_omega == omega && g->wtab32.ptr && g->wtab64.ptr) return;
+    const uint32_t rows = 1 + kTauTableRows, wpad = split_pad(omega);
+    std::vector<double> t(size_t(rows) * wpad, 0.0);
     for (uint32_t i = 1; i + 1 < omega; ++i) {
         const double lam = g->values[i];
-        const double sq = lam * lam;
-        t[i] = float(1.0 + lam);
+        const double sq = lam * lam, onem = 1 - lam;
+        t[i] = 1 + lam;
         double e = sq;
         for (uint32_t k = 0; k < uint32_t(kTauTableRows); ++k) {
-            t[size_t(k + 1) * omega + i] = float(e / (1.0 - lam));
+            t[size_t(k + 1) * wpad + i] = e / onem;
             e *= sq;
         }
     }
-    g->mixc.reserve(sizeof(float) * t.size());
-    TGTP_CUDA(cudaMemcpyAsync(g->mixc.ptr, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice,
-                              g->stream));
+    std::vector<float> tf(t.size());
+    for (size_t i = 0; i < t.size(); ++i) tf[i] = float(t[i]);
+    g->wtab64.reserve(sizeof(double) * t.size());
+    g->wtab32.reserve(sizeof(float) * tf.size());
+    TGTP_CUDA(cudaMemcpyAsync(g->wtab64.ptr, t.data(), sizeof(double) * t.size(),
+                              cudaMemcpyHostToDevice, g->stream));
+    TGTP_CUDA(cudaMemcpyAsync(g->wtab32.ptr, tf.data(), sizeof(float) * tf.size(),
+                              cudaMemcpyHostToDevice, g->stream));
     TGTP_CUDA(cudaStreamSynchronize(g->stream));
-    g->mix_omega = omega;
+    g->split_omega = omega;
+}
+
+// Row marks of this run: a fresh epoch per run, the marks zeroed when the buffers are first made
+// (and when the epoch counter wraps).
+RowMarks begin_row_marks(tgtp_graph* g) {
+    const size_t bytes = sizeof(uint32_t) * (g->n + 1);
+    if (!g->row_mark.ptr || g->row_mark.bytes < bytes) {
+        g->row_mark.reserve(bytes);
+        g->row_list.reserve(bytes);
+        TGTP_CUDA(cudaMemsetAsync(g->row_mark.ptr, 0, bytes, g->stream));
+        g->row_epoch = 0;
+    }
+    if (++g->row_epoch == 0) {
+        TGTP_CUDA(cudaMemsetAsync(g->row_mark.ptr, 0, bytes, g->stream));
+        g->row_epoch = 1;
+    }
+    RowMarks rm;
+    rm.mark = g->row_mark.as<uint32_t>();
+    rm.list = g->row_list.as<uint32_t>();
+    rm.len = run_work(g) + 2;
+    rm.epoch = g->row_epoch;
+    return rm;
 }
 
 // One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
@@ -1498,32 +1781,50 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
 
     g->taus.reserve(sizeof(int) * (m + 1));
     g->preds.reserve(sizeof(Acc) * (m + 1));
-    g->stats.reserve(sizeof(unsigned long long) * kStCount);
-    g->work.reserve(sizeof(unsigned) * 4);
+    // one zeroing for the striped counters and the work words behind them
+    const size_t stat_bytes = sizeof(unsigned long long) * kStCount * kStStripes;
+    g->stats.reserve(stat_bytes + sizeof(unsigned) * 4);
     auto* stats = g->stats.as<unsigned long long>();
-    auto* work = g->work.as<unsigned>();
-    TGTP_CUDA(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * kStCount, s));
-    TGTP_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned) * 4, s));
+    auto* work = run_work(g);
+    TGTP_CUDA(cudaMemsetAsync(stats, 0, stat_bytes + sizeof(unsigned) * 4, s));
 
-    if constexpr (JACOBI) {
-        prepare_mixed_tables(g, omega);
-        const Vec* vec = std::is_same<Vec, float>::value ? (const Vec*)g->vec_f32.ptr
-                                                          : (const Vec*)g->vec_bf16.ptr;
-        const uint64_t groups = (g->num_forward + 31) / 32;  // 32 edges per warp
+    const RowMarks rm = begin_row_marks(g);
+    if constexpr (JACOBI || std::is_same<Real, double>::value) {
+        // FP64 and mixed forms: eight lanes per edge over F64 / F32 / BF16 rows
+        prepare_split_tables(g, omega);
+        using Part = typename Split<Vec>::Part;
+        const Vec* vec = std::is_same<Vec, double>::value ? (const Vec*)g->vec_f64.ptr
+                         : std::is_same<Vec, float>::value ? (const Vec*)g->vec_f32.ptr
+                                                           : (const Vec*)g->vec_bf16.ptr;
+        const Part* wtab = std::is_same<Part, double>::value ? (const Part*)g->wtab64.ptr
+                                                             : (const Part*)g->wtab32.ptr;
+        const uint32_t wpad = split_pad(omega);
+        const size_t ssmem = 2 * sizeof(Part) * wpad;
+        int per_sm = 0;
+        TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tau_sums_kernel<Vec>, 256,
+                                                                ssmem));
+        if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel");
+        g->tau_sums.reserve(sizeof(double2) * (g->num_forward + 1));
+        const uint64_t need = (g->num_forward + 63) / 64;  // 64 edges per block and step
         const unsigned blocks = unsigned(std::max<uint64_t>(
-            1, std::min<uint64_t>((groups + 7) / 8, uint64_t(g->num_sms) * 8)));
-        ScopedKernel k(g->prof, s, "tau");
-        tau_mixed_kernel<Vec><<<blocks, 256, sizeof(float2) * omega, s>>>(
-            g->idx.as<uint32_t>(), g->adj.as<uint32_t>(), g->row_of.as<uint32_t>(),
-            g->rev.as<uint32_t>(), g->forward.as<uint32_t>(), g->num_forward, vec, g->omega, omega,
-            g->mixc.as<float>(), g->etab.as<double>(), g->onem.as<double>(), cfg.epsilon / 2.0,
-            double(m), c, g->taus.as<int>(), stats);
-        TGTP_LAUNCH_CHECK("tau_mixed_kernel");
+            1, std::min<uint64_t>(need, uint64_t(g->num_sms) * per_sm)));
+        {
+            ScopedKernel k(g->prof, s, "tau_sums");
+            tau_sums_kernel<Vec><<<blocks, 256, ssmem, s>>>(
+                g->fedge.as<uint4>(), g->num_forward, vec, g->omega, omega, wtab, wpad,
+                g->tau_sums.as<double2>());
+            TGTP_LAUNCH_CHECK("tau_sums_kernel");
+        }
+        ScopedKernel k(g->prof, s, "tau_bound");
+        tau_bound_kernel<Vec><<<grid_cap(g->num_forward, 256, g->num_sms, 8), 256, 0, s>>>(
+            g->fedge.as<uint4>(), g->deg.as<uint32_t>(), g->num_forward,
+            g->tau_sums.as<double2>(), vec, g->omega, omega, wtab, wpad, g->etab.as<double>(),
+            g->onem.as<double>(), cfg.epsilon / 2.0, m, c, g->taus.as<int>(), rm, stats);
+        TGTP_LAUNCH_CHECK("tau_bound_kernel");
     } else {
-        const Real* vec = std::is_same<Real, float>::value ? (const Real*)g->vec_f32.ptr
-                                                            : (const Real*)g->vec_f64.ptr;
-        const Real* etab = std::is_same<Real, float>::value ? (const Real*)g->etab_f.ptr
-                                                             : (const Real*)g->etab.ptr;
+        // FP32 form: the reference's arithmetic and summation order
+        const Real* vec = (const Real*)g->vec_f32.ptr;
+        const Real* etab = (const Real*)g->etab_f.ptr;
         const Real eps_half = Real(cfg.epsilon / 2.0);
         // per block: two double2 constants per index; per warp: two buffers of (x_u, x_v) chunks
         // of 32 edges x one 128-byte row piece, rows padded by one element
@@ -1545,7 +1846,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             g->idx.as<uint32_t>(), g->adj.as<uint32_t>(), g->row_of.as<uint32_t>(),
             g->rev.as<uint32_t>(), g->forward.as<uint32_t>(), g->num_forward, vec, g->omega, omega,
             g->onep.as<double>(), g->onem.as<double>(), etab, g->etab.as<double>(), eps_half, m, c,
-            g->taus.as<int>(), stats);
+            g->taus.as<int>(), rm, stats);
         TGTP_LAUNCH_CHECK("tau_kernel");
     }
 
@@ -1589,6 +1890,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.taus = g->taus.as<int>();
     p.preds = g->preds.as<Acc>();
     p.work = work;
+    p.rows = rm.list;
     p.qbuf = reinterpret_cast<uint32_t*>(base);
     base += q_bytes;
     p.items = reinterpret_cast<WalkItem*>(base);
@@ -1604,7 +1906,6 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.eps = cfg.epsilon;
     p.logmd = logmd;
     p.gamma = cfg.gamma;
-    p.ell_out = nullptr;
     p.stats = stats;
     p.adjd = g->adjd.as<uint2>();
     p.budget_ns = deadline_from_env();
@@ -1614,10 +1915,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         TGTP_LAUNCH_CHECK("source_kernel");
     }
     {
-        ScopedKernel k(g->prof, s, "symmetrize");
-        symmetrize_kernel<Acc><<<grid_cap(m, 256, g->num_sms, 8), 256, 0, s>>>(
-            g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), m, out);
-        TGTP_LAUNCH_CHECK("symmetrize_kernel");
+        ScopedKernel k(g->prof, s, "finish");
+        finish_kernel<Real, Acc><<<grid_cap(m, 256, g->num_sms, 8), 256, 0, s>>>(
+            g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), g->row_of.as<uint32_t>(),
+            g->adjd.as<uint2>(), g->deg.as<uint32_t>(), rm.mark, rm.epoch, m, out, stats);
+        TGTP_LAUNCH_CHECK("finish_kernel");
     }
 }
 
@@ -1672,7 +1974,7 @@ using namespace tgtp;
 namespace {
 void finish_run(tgtp_graph* g) {
     unsigned flags[2];
-    TGTP_CUDA(cudaMemcpyAsync(flags, g->work.ptr, sizeof(flags), cudaMemcpyDeviceToHost, g->stream));
+    TGTP_CUDA(cudaMemcpyAsync(flags, run_work(g), sizeof(flags), cudaMemcpyDeviceToHost, g->stream));
     TGTP_CUDA(cudaStreamSynchronize(g->stream));
     if (flags[1] & kErrDeadline)
         fail(TGTP_ERR_TIMEOUT, "device time budget exceeded (TGTP_KERNEL_DEADLINE_S)");
@@ -1707,9 +2009,13 @@ tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out) {
         if (!g || !out) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
         if (!g->have_run) fail(TGTP_ERR_INVALID_ARGUMENT, "no run on this graph yet");
         finish_run(g);
-        unsigned long long st[kStCount];
-        TGTP_CUDA(cudaMemcpyAsync(st, g->stats.ptr, sizeof(st), cudaMemcpyDeviceToHost, g->stream));
+        unsigned long long stripes[kStCount * kStStripes];
+        TGTP_CUDA(cudaMemcpyAsync(stripes, g->stats.ptr, sizeof(stripes), cudaMemcpyDeviceToHost,
+                                  g->stream));
         TGTP_CUDA(cudaStreamSynchronize(g->stream));
+        unsigned long long st[kStCount] = {};
+        for (int c = 0; c < kStStripes; ++c)
+            for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
         out->push_rounds = st[kStPushRounds];
         out->push_vertices = st[kStPushVertices];
         out->push_traversals = st[kStPushTraversals];

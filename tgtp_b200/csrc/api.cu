@@ -230,11 +230,12 @@ __global__ void adjd_kernel(const uint32_t* __restrict__ adj, const uint32_t* __
 // forward slots (v >= u) are the tail of each sorted row; count them per row.
 __global__ void forward_count_kernel(const uint32_t* __restrict__ idx,
                                      const uint32_t* __restrict__ adj, uint64_t n,
-                                     uint32_t* __restrict__ cnt) {
+                                     uint32_t* __restrict__ cnt, uint32_t* __restrict__ lbp) {
     for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < n;
          u += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t lb = lower_bound_u32(adj, idx[u], idx[u + 1], uint32_t(u));
         cnt[u] = idx[u + 1] - lb;
+        lbp[u] = lb;
     }
 }
 
@@ -277,14 +278,21 @@ __global__ void scan_kernel(uint32_t* __restrict__ cnt, uint64_t n, uint32_t* __
     if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void forward_fill_kernel(const uint32_t* __restrict__ idx,
-                                    const uint32_t* __restrict__ adj, uint64_t n,
-                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ fwd) {
-    for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < n;
-         u += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t lb = lower_bound_u32(adj, idx[u], idx[u + 1], uint32_t(u));
-        const uint32_t o = off[u];
-        for (uint32_t p = lb; p < idx[u + 1]; ++p) fwd[o + (p - lb)] = p;
+// One thread per slot: forward slot p = (u, v >= u) goes to off[u] + (p - lb[u]), with the edge's
+// record (u, v, p, reverse slot of p) beside it for the tau kernels.
+__global__ void forward_fill_kernel(const uint32_t* __restrict__ adj,
+                                    const uint32_t* __restrict__ row_of,
+                                    const uint32_t* __restrict__ rev, uint64_t m,
+                                    const uint32_t* __restrict__ off,
+                                    const uint32_t* __restrict__ lbp, uint32_t* __restrict__ fwd,
+                                    uint4* __restrict__ fedge) {
+    for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < m;
+         p += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t u = row_of[p], v = adj[p];
+        if (v < u) continue;
+        const uint32_t e = off[u] + (uint32_t(p) - lbp[u]);
+        fwd[e] = uint32_t(p);
+        fedge[e] = make_uint4(u, v, uint32_t(p), rev[p]);
     }
 }
 
@@ -336,10 +344,12 @@ void graph_prepare(tgtp_graph* g) {
         TGTP_LAUNCH_CHECK("adjd_kernel");
     }
     // forward slot list
-    DeviceBuffer cnt;
+    DeviceBuffer cnt, lbp;
     cnt.reserve(sizeof(uint32_t) * (n + 2));
+    lbp.reserve(sizeof(uint32_t) * (n + 1));
     auto* c = cnt.as<uint32_t>();
-    forward_count_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c);
+    forward_count_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c,
+                                                                 lbp.as<uint32_t>());
     TGTP_LAUNCH_CHECK("forward_count_kernel");
     scan_kernel<<<1, 1024, 0, s>>>(c, n, c + n + 1);
     TGTP_LAUNCH_CHECK("scan_kernel");
@@ -348,8 +358,11 @@ void graph_prepare(tgtp_graph* g) {
     TGTP_CUDA(cudaStreamSynchronize(s));
     g->num_forward = total;
     g->forward.reserve(sizeof(uint32_t) * (total + 1));
-    forward_fill_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c,
-                                                                g->forward.as<uint32_t>());
+    g->fedge.reserve(sizeof(uint4) * (total + 1));
+    if (m)
+        forward_fill_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(
+            adj, g->row_of.as<uint32_t>(), g->rev.as<uint32_t>(), m, c, lbp.as<uint32_t>(),
+            g->forward.as<uint32_t>(), g->fedge.as<uint4>());
     TGTP_LAUNCH_CHECK("forward_fill_kernel");
     TGTP_CUDA(cudaStreamSynchronize(s));
 }
@@ -464,7 +477,7 @@ tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* 
         cudaStream_t s = g->stream;
         const uint64_t count = g->n * uint64_t(omega);
         g->omega = omega;
-        g->mix_omega = 0;
+        g->split_omega = 0;
         g->values.assign(values, values + omega);
         g->d_values.reserve(sizeof(double) * omega);
         TGTP_CUDA(cudaMemcpyAsync(g->d_values.ptr, values, sizeof(double) * omega,

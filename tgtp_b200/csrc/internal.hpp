@@ -156,6 +156,7 @@ struct tgtp_graph {
     tgtp::DeviceBuffer rev;      // slot (u,v) -> lower_bound of u in row v
     tgtp::DeviceBuffer sym_src;  // slot q -> 1 + last slot p with rev[p] == q (0: none)
     tgtp::DeviceBuffer forward;  // slots with v >= u, in CSR order
+    tgtp::DeviceBuffer fedge;    // per forward slot: (u, v, slot, reverse slot)
     tgtp::DeviceBuffer adjd;     // slot -> (neighbour, neighbour's degree)
 
     // eigenpairs
@@ -165,12 +166,15 @@ struct tgtp_graph {
     // tau-bound constants: onep[i] = 1 + lambda_i, onem[i] = 1 - lambda_i and the powers
     // lambda_i^(2(k+1)) for k < kTauTableRows, formed by the reference's repeated multiplication
     tgtp::DeviceBuffer onep, onem, etab, etab_f;
-    tgtp::DeviceBuffer mixc;     // FP32 weights of the mixed tau kernel for mix_omega
-    uint32_t mix_omega = 0;
+    tgtp::DeviceBuffer wtab32, wtab64;  // weights of the split tau kernel for split_omega
+    uint32_t split_omega = 0;
+    tgtp::DeviceBuffer row_mark, row_list;  // rows with a slot of tau > 1 (this run's epoch)
+    uint32_t row_epoch = 0;
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
-    tgtp::DeviceBuffer taus, preds, stats, counters, sums, work, scratch, out;
+    tgtp::DeviceBuffer taus, preds, stats, counters, sums, scratch, out;
+    tgtp::DeviceBuffer tau_sums;  // per forward edge: (upsilon, delta_0) sums of the split forms
     int32_t last_precision = -1;
     bool have_run = false;
 
