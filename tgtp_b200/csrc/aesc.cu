@@ -76,6 +76,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
+// Programmatic dependent launch: a kernel lets the next one in the stream start its blocks early
+// (launch_dependents) and the next one waits for it to finish, with its memory visible, before it
+// touches its results (wait).  Without the launch attribute wait returns at once.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // get_tau (src/aesc.h:129-135).  p1/p2 in the reference's parameter order (its callers pass
 // (degree(u), degree(v)) into parameters named (dv, du)).  The 1 - lambda^2 and log(1/|lambda|)
 // constants are formed on the host with the same libm as the reference.
@@ -177,6 +185,7 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
     constexpr uint32_t CH = 128 / sizeof(Real);  // chunk: one 128-byte row piece
     constexpr uint32_t LD = CH + 1;              // odd tile stride: conflict-free own-row reads
     extern __shared__ __align__(16) unsigned char tsm[];
+    pdl_launch_dependents();
     const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t wpb = blockDim.x >> 5;
     // per index: (1 + lambda_i, 1 - lambda_i) and (RN(1 / (1 - lambda_i)), eigen_t_1 row 0)
@@ -490,6 +499,7 @@ tau_sums_kernel(const uint4* __restrict__ fedge, uint64_t num_forward, const Vec
                 uint32_t wpad, double2* __restrict__ sums) {
     using Part = typename Split<Vec>::Part;
     extern __shared__ __align__(16) unsigned char ssm[];
+    pdl_launch_dependents();
     Part* wu = reinterpret_cast<Part*>(ssm);  // upsilon weights, then delta_0 weights
     Part* wd = wu + wpad;
     for (uint32_t i = threadIdx.x; i < 2 * wpad; i += blockDim.x) wu[i] = __ldg(wtab + i);
@@ -543,6 +553,8 @@ tau_bound_kernel(const uint4* __restrict__ fedge, const uint32_t* __restrict__ d
     const double mdbl = double(m);
     const double inv_b1 = 1.0 / c.b1, inv_b2 = 1.0 / c.b2;
     unsigned long long iters = 0, ambiguous = 0;
+    pdl_launch_dependents();
+    pdl_wait();  // the sums of tau_sums_kernel
     for (uint64_t base = gw * 32; base < num_forward; base += nw * 32) {
         const uint64_t e = base + lane;
         const bool act = e < num_forward;
@@ -894,6 +906,8 @@ source_kernel(SourceParams<Real, Acc> p) {
     };
     __syncwarp();
 
+    pdl_launch_dependents();
+    pdl_wait();  // taus, row list and its length from the tau kernels
     const unsigned nrows = p.work[2];  // final: the tau kernel that appends to the list has ended
     // list entry gw first, then entries past the grid's warps claimed one at a time (warps past
     // the list's end leave without touching the counter)
@@ -1662,6 +1676,7 @@ finish_kernel(const Acc* __restrict__ preds, const uint32_t* __restrict__ sym_sr
               const uint32_t* __restrict__ deg, const uint32_t* __restrict__ mark, uint32_t epoch,
               uint64_t m, float* __restrict__ out, unsigned long long* __restrict__ stats) {
     unsigned long long rows = 0, trav = 0;
+    pdl_wait();  // pre-symmetric scores of the source kernel
     for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < m;
          q += uint64_t(gridDim.x) * blockDim.x) {
         // first level: the slot's row, its (neighbour, degree) and the slot landing on it
@@ -1763,6 +1778,32 @@ RowMarks begin_row_marks(tgtp_graph* g) {
     return rm;
 }
 
+// Kernel launch on the handle's stream; with pdl the launch may begin while the previous kernel
+// finishes (the kernel waits for it with pdl_wait).  TGTP_PDL=0 turns the overlap off.
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("TGTP_PDL");
+        return !(e && std::string(e) == "0");
+    }();
+    return on;
+}
+
+template <class... KArgs, class... Args>
+void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+            bool pdl, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = (pdl && pdl_enabled()) ? 1 : 0;
+    TGTP_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 // One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
 // JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
 template <class Real, class Acc, bool JACOBI, class Vec>
@@ -1810,14 +1851,14 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             1, std::min<uint64_t>(need, uint64_t(g->num_sms) * per_sm)));
         {
             ScopedKernel k(g->prof, s, "tau_sums");
-            tau_sums_kernel<Vec><<<blocks, 256, ssmem, s>>>(
+            launch(tau_sums_kernel<Vec>, blocks, 256, ssmem, s, false,
                 g->fedge.as<uint4>(), g->num_forward, vec, g->omega, omega, wtab, wpad,
                 g->tau_sums.as<double2>());
             TGTP_LAUNCH_CHECK("tau_sums_kernel");
         }
         ScopedKernel k(g->prof, s, "tau_bound");
-        tau_bound_kernel<Vec><<<grid_cap(g->num_forward, 256, g->num_sms, 8), 256, 0, s>>>(
-            g->fedge.as<uint4>(), g->deg.as<uint32_t>(), g->num_forward,
+        launch(tau_bound_kernel<Vec>, grid_cap(g->num_forward, 256, g->num_sms, 8), 256, 0, s,
+            true, g->fedge.as<uint4>(), g->deg.as<uint32_t>(), g->num_forward,
             g->tau_sums.as<double2>(), vec, g->omega, omega, wtab, wpad, g->etab.as<double>(),
             g->onem.as<double>(), cfg.epsilon / 2.0, m, c, g->taus.as<int>(), rm, stats);
         TGTP_LAUNCH_CHECK("tau_bound_kernel");
@@ -1911,12 +1952,12 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.budget_ns = deadline_from_env();
     {
         ScopedKernel k(g->prof, s, "source");
-        kern<<<unsigned(blocks), threads, smem, s>>>(p);
+        launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
         TGTP_LAUNCH_CHECK("source_kernel");
     }
     {
         ScopedKernel k(g->prof, s, "finish");
-        finish_kernel<Real, Acc><<<grid_cap(m, 256, g->num_sms, 8), 256, 0, s>>>(
+        launch(finish_kernel<Real, Acc>, grid_cap(m, 256, g->num_sms, 8), 256, 0, s, true,
             g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), g->row_of.as<uint32_t>(),
             g->adjd.as<uint2>(), g->deg.as<uint32_t>(), rm.mark, rm.epoch, m, out, stats);
         TGTP_LAUNCH_CHECK("finish_kernel");
