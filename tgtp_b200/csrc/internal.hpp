@@ -175,6 +175,9 @@ struct tgtp_graph {
     // run scratch
     tgtp::DeviceBuffer taus, preds, stats, counters, sums, scratch, out;
     tgtp::DeviceBuffer tau_sums;  // per forward edge: (upsilon, delta_0) sums of the split forms
+    // walk copy of the graph renumbered by degree (built on the first saba_count)
+    tgtp::DeviceBuffer saba_info, saba_adj, saba_cnt;
+    bool saba_ready = false;
     int32_t last_precision = -1;
     bool have_run = false;
 

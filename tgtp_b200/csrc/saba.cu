@@ -13,7 +13,12 @@
 // `hot` live in shared memory per block (hubs have low ids in the power-law generators, and every
 // id is hot when n is small) and are flushed once at the end; the rest go to L2 atomics.
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
+#include <string>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -100,6 +105,154 @@ saba_walk_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ 
     if (lane == 0 && f) atomicAdd(fallback_total, (unsigned long long)f);
 }
 
+// ---- walk graph renumbered by degree ---------------------------------------------------------------
+// A walk visits a vertex in proportion to its degree, so the counters that take most increments
+// belong to the highest-degree vertices.  saba_count renumbers the vertices by degree (highest
+// first, ties by id) into a walk copy of the graph: row p holds the neighbours of vertex orig(p) in
+// their original order, renumbered, and info[p] = (row start, degree, orig(p), 0) is one 16-byte
+// load per hop.  The hash of the primary phase and the neighbour index k are taken on the original
+// ids and orders, so every trajectory is the reference's; the counters of the first `hot` numbers
+// live in shared memory, and the per-number counters are scattered back to the original ids at the
+// end.
+__global__ void saba_iota_kernel(uint32_t* __restrict__ ids, uint64_t n) {
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+         v += uint64_t(gridDim.x) * blockDim.x)
+        ids[v] = uint32_t(v);
+}
+
+__global__ void saba_info_kernel(const uint32_t* __restrict__ order, const uint32_t* __restrict__ sdeg,
+                                 const uint32_t* __restrict__ beg, uint64_t n,
+                                 uint4* __restrict__ info, uint32_t* __restrict__ inv) {
+    for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
+         p += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t old = order[p];
+        info[p] = make_uint4(beg[p], sdeg[p], old, 0u);
+        inv[old] = uint32_t(p);
+    }
+}
+
+__global__ void saba_adj_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
+                                const uint32_t* __restrict__ row_of,
+                                const uint32_t* __restrict__ inv, const uint4* __restrict__ info,
+                                uint64_t m, uint32_t* __restrict__ adjp) {
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < m;
+         q += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t old = row_of[q];
+        const uint32_t p = inv[old];
+        adjp[info[p].x + (uint32_t(q) - idx[old])] = inv[adj[q]];
+    }
+}
+
+__global__ void saba_scatter_kernel(const uint32_t* __restrict__ cnt, const uint4* __restrict__ info,
+                                    uint64_t n, uint32_t* __restrict__ counters) {
+    for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
+         p += uint64_t(gridDim.x) * blockDim.x)
+        counters[info[p].z] = cnt[p];
+}
+
+// The walk on the renumbered graph.  Each lane carries WPL walkers (bouquets 4w + g of the warp's
+// step, g = lane / 8) whose hops are interleaved, so WPL independent load chains are in flight per
+// lane.  A warp takes a contiguous, equal share of the steps (4 WPL bouquets each).
+template <int WPL>
+__global__ void __launch_bounds__(kSabaThreads)
+saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict__ adjp,
+                      uint32_t depth, uint32_t bouquets_per_src, uint32_t grid_step,
+                      uint64_t total_bouquets, uint32_t* __restrict__ cnt, uint32_t hot,
+                      unsigned long long* __restrict__ fallback_total) {
+    extern __shared__ uint32_t s_cnt[];
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+
+    const uint32_t lane = threadIdx.x & 31, j = lane & 7, grp = lane >> 3;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    constexpr uint32_t SB = 4 * WPL;  // bouquets per warp step
+    const uint64_t steps = (total_bouquets + SB - 1) / SB;
+    const uint64_t s_lo = steps * warp / nwarps, s_hi = steps * (warp + 1) / nwarps;
+
+    uint32_t src[WPL], bq[WPL];
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) {
+        const uint64_t b = s_lo * SB + uint32_t(w) * 4 + grp;
+        src[w] = uint32_t(b / bouquets_per_src);
+        bq[w] = uint32_t(b - uint64_t(src[w]) * bouquets_per_src);
+    }
+    uint32_t fallbacks = 0;
+    for (uint64_t st = s_lo; st < s_hi; ++st) {
+        bool active[WPL], primary[WPL];
+        uint32_t beg[WPL], d[WPL], orig[WPL], secret[WPL], state[WPL];
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) {
+            const uint64_t b = st * SB + uint32_t(w) * 4 + grp;
+            active[w] = b < total_bouquets;
+            beg[w] = d[w] = orig[w] = 0;
+            if (active[w]) {
+                const uint4 r = __ldg(info + src[w]);
+                beg[w] = r.x;
+                d[w] = r.y;
+                orig[w] = r.z;
+                active[w] = r.y != 0;  // isolated sources are skipped (:197-198)
+            }
+            secret[w] = (bq[w] * 8u + j + 1u) * grid_step;
+            state[w] = secret[w];
+            primary[w] = true;
+        }
+        for (uint32_t len = 0; len < depth; ++len) {
+            uint32_t nxt[WPL];
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                const unsigned zero =
+                    __ballot_sync(kFullMask, active[w] && primary[w] && secret[w] == 0u);
+                if ((zero >> (grp * 8)) & 0xffu) primary[w] = false;
+            }
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                nxt[w] = 0;
+                if (active[w]) {
+                    uint32_t k;
+                    if (primary[w]) {
+                        k = __umulhi(secret[w] ^ fmix32(orig[w]), d[w]);
+                        secret[w] *= d[w];
+                    } else {
+                        k = splitmix32(state[w]) % d[w];
+                    }
+                    nxt[w] = __ldg(adjp + beg[w] + k);
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                if (active[w]) {
+                    const uint4 r = __ldg(info + nxt[w]);
+                    beg[w] = r.x;
+                    d[w] = r.y;
+                    orig[w] = r.z;
+                    if (nxt[w] < hot) atomicAdd(s_cnt + nxt[w], 1u);
+                    else atomicAdd(cnt + nxt[w], 1u);
+                }
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) {
+            if (active[w] && !primary[w] && j == 0) ++fallbacks;
+            bq[w] += SB;
+            while (bq[w] >= bouquets_per_src) {
+                bq[w] -= bouquets_per_src;
+                ++src[w];
+            }
+        }
+    }
+
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
+        const uint32_t c = s_cnt[i];
+        if (c) atomicAdd(cnt + i, c);
+    }
+    uint32_t f = fallbacks;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) f += __shfl_xor_sync(kFullMask, f, o);
+    if (lane == 0 && f) atomicAdd(fallback_total, (unsigned long long)f);
+}
+
 // visit_count = sum c[v], checksum = sum (v+1) c[v], both exact in 64 bits.
 __global__ void saba_sums_kernel(const uint32_t* __restrict__ c, uint64_t n,
                                  unsigned long long* __restrict__ out) {
@@ -123,6 +276,76 @@ __global__ void saba_sums_kernel(const uint32_t* __restrict__ c, uint64_t n,
 
 }  // namespace
 
+// Builds the degree-renumbered walk copy of the graph once per handle.
+void saba_prepare(tgtp_graph* g) {
+    if (g->saba_ready) return;
+    cudaStream_t s = g->stream;
+    const uint64_t n = g->n, m = g->m;
+    if (n > uint64_t(INT32_MAX) || m > uint64_t(UINT32_MAX))
+        fail(TGTP_ERR_UNSUPPORTED, "graph too large for the walk counter");
+    g->saba_info.reserve(sizeof(uint4) * (n + 1));
+    g->saba_adj.reserve(sizeof(uint32_t) * (m + 1));
+    DeviceBuffer ids, order, sdeg, beg, inv, tmp;
+    ids.reserve(sizeof(uint32_t) * (n + 1));
+    order.reserve(sizeof(uint32_t) * (n + 1));
+    sdeg.reserve(sizeof(uint32_t) * (n + 1));
+    beg.reserve(sizeof(uint32_t) * (n + 1));
+    inv.reserve(sizeof(uint32_t) * (n + 1));
+    const unsigned nb = unsigned(std::min<uint64_t>((n + 255) / 256, 8u * g->num_sms));
+    saba_iota_kernel<<<nb ? nb : 1, 256, 0, s>>>(ids.as<uint32_t>(), n);
+    TGTP_LAUNCH_CHECK("saba_iota_kernel");
+    size_t t1 = 0, t2 = 0;
+    TGTP_CUDA(cub::DeviceRadixSort::SortPairsDescending(
+        nullptr, t1, g->deg.as<uint32_t>(), sdeg.as<uint32_t>(), ids.as<uint32_t>(),
+        order.as<uint32_t>(), int(n), 0, 32, s));
+    TGTP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, sdeg.as<uint32_t>(), beg.as<uint32_t>(),
+                                            int(n), s));
+    tmp.reserve(std::max(t1, t2));
+    TGTP_CUDA(cub::DeviceRadixSort::SortPairsDescending(
+        tmp.ptr, t1, g->deg.as<uint32_t>(), sdeg.as<uint32_t>(), ids.as<uint32_t>(),
+        order.as<uint32_t>(), int(n), 0, 32, s));
+    TGTP_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, t2, sdeg.as<uint32_t>(), beg.as<uint32_t>(),
+                                            int(n), s));
+    saba_info_kernel<<<nb ? nb : 1, 256, 0, s>>>(order.as<uint32_t>(), sdeg.as<uint32_t>(),
+                                                 beg.as<uint32_t>(), n, g->saba_info.as<uint4>(),
+                                                 inv.as<uint32_t>());
+    TGTP_LAUNCH_CHECK("saba_info_kernel");
+    if (m) {
+        const unsigned mb = unsigned(std::min<uint64_t>((m + 255) / 256, 8u * g->num_sms));
+        saba_adj_kernel<<<mb, 256, 0, s>>>(g->idx.as<uint32_t>(), g->adj.as<uint32_t>(),
+                                           g->row_of.as<uint32_t>(), inv.as<uint32_t>(),
+                                           g->saba_info.as<uint4>(), m, g->saba_adj.as<uint32_t>());
+        TGTP_LAUNCH_CHECK("saba_adj_kernel");
+    }
+    TGTP_CUDA(cudaStreamSynchronize(s));  // the temporaries go back to the cache
+    g->saba_ready = true;
+}
+
+template <int WPL>
+void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step, uint64_t total,
+                 uint32_t* cnt, unsigned long long* fb) {
+    cudaStream_t s = g->stream;
+    uint32_t cap = kSabaHotCap;
+    if (const char* e = std::getenv("TGTP_SABA_HOT")) cap = uint32_t(std::atoi(e));
+    cap = std::max<uint32_t>(1024u, std::min<uint32_t>(cap, 53248u));
+    const uint32_t hot = uint32_t(g->n < cap ? g->n : cap);
+    const size_t smem = sizeof(uint32_t) * hot;
+    TGTP_CUDA(cudaFuncSetAttribute(saba_walk_perm_kernel<WPL>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, saba_walk_perm_kernel<WPL>,
+                                                            kSabaThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = uint64_t(g->num_sms) * per_sm;
+    const uint64_t need = (total + 4 * WPL - 1) / (4 * WPL) / (kSabaThreads / 32) + 1;
+    if (blocks > need) blocks = need;
+    ScopedKernel k(g->prof, s, "saba_walk");
+    saba_walk_perm_kernel<WPL><<<unsigned(blocks), kSabaThreads, smem, s>>>(
+        g->saba_info.as<uint4>(), g->saba_adj.as<uint32_t>(), depth, bps, grid_step, total, cnt,
+        hot, fb);
+    TGTP_LAUNCH_CHECK("saba_walk_perm_kernel");
+}
+
 void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_counters) {
     cudaStream_t s = g->stream;
     g->sums.reserve(4 * sizeof(unsigned long long));
@@ -130,26 +353,26 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
     TGTP_CUDA(cudaMemsetAsync(device_counters, 0, sizeof(uint32_t) * g->n, s));
     TGTP_CUDA(cudaMemsetAsync(sums, 0, 4 * sizeof(unsigned long long), s));
     if (n_walks == 0 || depth == 0) return;
+    saba_prepare(g);
     const uint32_t bouquets_per_src = n_walks / 8;
     const uint32_t grid_step = UINT32_MAX / n_walks;
     const uint64_t total = g->n * uint64_t(bouquets_per_src);
-    const uint32_t hot = uint32_t(g->n < kSabaHotCap ? g->n : kSabaHotCap);
-    const size_t smem = sizeof(uint32_t) * hot;
-    TGTP_CUDA(cudaFuncSetAttribute(saba_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(sizeof(uint32_t) * kSabaHotCap)));
-    int per_sm = 0;
-    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, saba_walk_kernel,
-                                                            kSabaThreads, smem));
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = uint64_t(g->num_sms) * per_sm;
-    const uint64_t need = (total + 3) / 4 / (kSabaThreads / 32) + 1;  // one group-step per warp
-    if (blocks > need) blocks = need;
+    g->saba_cnt.reserve(sizeof(uint32_t) * (g->n + 1));
+    auto* cnt = g->saba_cnt.as<uint32_t>();
+    TGTP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * g->n, s));
+    int wpl = 1;
+    if (const char* e = std::getenv("TGTP_SABA_WPL")) wpl = std::atoi(e);
+    switch (wpl) {
+        case 2: saba_launch<2>(g, depth, bouquets_per_src, grid_step, total, cnt, sums + 2); break;
+        case 4: saba_launch<4>(g, depth, bouquets_per_src, grid_step, total, cnt, sums + 2); break;
+        default: saba_launch<1>(g, depth, bouquets_per_src, grid_step, total, cnt, sums + 2); break;
+    }
     {
-        ScopedKernel k(g->prof, s, "saba_walk");
-        saba_walk_kernel<<<unsigned(blocks), kSabaThreads, smem, s>>>(
-            g->idx.as<uint32_t>(), g->adj.as<uint32_t>(), depth, bouquets_per_src, grid_step, total,
-            device_counters, hot, sums + 2);
-        TGTP_LAUNCH_CHECK("saba_walk_kernel");
+        ScopedKernel k(g->prof, s, "saba_scatter");
+        const unsigned nb = unsigned(std::min<uint64_t>((g->n + 255) / 256, 8u * g->num_sms));
+        saba_scatter_kernel<<<nb ? nb : 1, 256, 0, s>>>(cnt, g->saba_info.as<uint4>(), g->n,
+                                                        device_counters);
+        TGTP_LAUNCH_CHECK("saba_scatter_kernel");
     }
 }
 
