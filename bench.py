@@ -133,6 +133,53 @@ def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int
     return secs
 
 
+def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
+    """SABA walk counter at scale: seeded R-MAT scale 18, edge factor 16 (a=0.57, b=c=0.19), largest
+    component; depth 5, 2048 walks per vertex.  Kernel time from the library's CUDA events (3 runs
+    after 1 warm-up); transitions = active vertices x walks x depth; 20 algorithmic bytes per
+    transition (idx pair 8, adj 4, counter read + write 8).  The reference's rw_experiment_saba,
+    built from its sources, timed once on the host cores beside it."""
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    g = synth.config3_graph(1)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    saba_count(dg, 5, 2048, counters=False)
+    dg.set_profiling(True)
+    for _ in range(3):
+        _, vc, cs, fb = saba_count(dg, 5, 2048, counters=False)
+    ks = dg.kernel_stats()
+    dg.set_profiling(False)
+    dg.free()
+    ms = ks["saba_walk"][1] / ks["saba_walk"][0]
+    trans = g.n * 2048 * 5
+    out = {"workload": f"SABA d5 w2048 on R-MAT scale 18 (LCC n={g.n}, E={g.num_edges})",
+           "transitions_per_s": trans / (ms * 1e-3), "kernel_ms": ms,
+           "kernel_ms_all": {k: v[1] / v[0] for k, v in ks.items()},
+           "hbm_frac_of_" + peak_kind: trans * 20 / (ms * 1e-3) / 1e9 / hbm,
+           "visit_count": vc, "checksum": cs, "fallback_bouquets": fb}
+    if with_cpu:
+        import oracle
+
+        exe = oracle.ref_binary("rw_experiment_saba")
+        if exe is not None:
+            folder = os.path.join(root, "saba_data")
+            os.makedirs(os.path.join(folder, "rmat18"), exist_ok=True)
+            synth.write_graph_txt(g, os.path.join(folder, "rmat18", "graph.txt"))
+            threads = os.cpu_count() or 1
+            r = subprocess.run([exe, folder, "rmat18", "5", "2048", str(threads)],
+                               capture_output=True, text=True, cwd=root, timeout=900,
+                               env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+            if r.returncode == 0:
+                f = r.stdout.strip().splitlines()[-1].split("\t")
+                out["cpu_reference"] = {"transitions_per_s": float(f[11]) * 5, "cores": threads,
+                                        "walk_seconds": float(f[8]),
+                                        "sample": "one run of the reference rw_experiment_saba "
+                                                  "(-Ofast, OpenMP) on the same graph"}
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -171,6 +218,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rmat", action="store_true", help="skip the R-MAT scale-18 walk line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -245,14 +293,18 @@ def main():
 
     # ---- headline: FP64 form, inputs resident ----
     with ClockSampler(local) as clocks:
-        ms64, wall64, k64, st64 = timed(PRECISION_FP64, args.steps, args.warmup, True)
-    out64 = out.clone()
+        ms64, wall64, _, st64 = timed(PRECISION_FP64, args.steps, args.warmup, False)
+    # per-kernel CUDA events (they sit between the kernels, so they are taken on a separate pass)
     side_steps = max(args.steps // 4, 10)
-    ms32, _, k32, st32 = timed(PRECISION_FP32, side_steps, args.warmup, True)
+    _, _, k64, _ = timed(PRECISION_FP64, side_steps, args.warmup, True)
+    out64 = out.clone()
+    ms32, _, _, _ = timed(PRECISION_FP32, side_steps, args.warmup, False)
+    _, _, k32, _ = timed(PRECISION_FP32, side_steps, args.warmup, True)
     mixed = {}
     for label, vec in (("mixed_f32_vectors", VEC_F32), ("mixed_bf16_vectors", VEC_BF16)):
-        msx, _, kx, _ = timed(PRECISION_MIXED, side_steps, args.warmup, True, vec)
+        msx, _, _, _ = timed(PRECISION_MIXED, side_steps, args.warmup, False, vec)
         dev = (out.double() - out64.double()).abs() / out64.double().abs()
+        _, _, kx, _ = timed(PRECISION_MIXED, side_steps, args.warmup, True, vec)
         mixed[label] = {"ms_per_step": msx / side_steps,
                         "kernel_ms": {k: v[1] / v[0] for k, v in kx.items()},
                         "max_rel_dev_vs_fp64": float(dev.max())}
@@ -338,6 +390,8 @@ def main():
         saba = {"workload": "SABA d5 w2048 on the same graph", "transitions_per_s":
                 trans / (saba_ms * 1e-3), "kernel_ms": saba_ms,
                 "hbm_frac_of_" + peak_kind: trans * 20 / (saba_ms * 1e-3) / 1e9 / hbm}
+        if not args.no_rmat:
+            saba["rmat18"] = saba_rmat18(hbm, peak_kind, root, not args.no_cpu_baseline)
 
         cpu = None
         if not args.no_cpu_baseline:
@@ -363,9 +417,10 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "matches_resident_run": ok_e2e},
-            "gpu_launches": int(sum(v[0] for v in k64.values())),
+            # the library's kernels per step (from the event pass) times the timed steps
+            "gpu_launches": int(round(sum(v[0] for v in k64.values()) / side_steps)) * args.steps,
             # cross-check: the library's own per-kernel events, summed per step (<= ms_per_step)
-            "kernel_ms_sum_per_step": sum(v[1] for v in k64.values()) / args.steps,
+            "kernel_ms_sum_per_step": sum(v[1] for v in k64.values()) / side_steps,
             "clocks": clocks.summary(),
             "forms": {"fp64": {"edges_per_s": value / world, "ms_per_step": ms_step},
                       "fp32_reference_arithmetic": {"edges_per_s": E / (ms32 / side_steps * 1e-3),
