@@ -147,6 +147,32 @@ tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out);
 /* Per-slot tau of the last run (m int32, host). */
 tgtp_status tgtp_last_taus(tgtp_graph* g, int32_t* host_taus);
 
+/* Times the candidate layouts of the source kernel (per-source residual vectors in shared memory
+ * or in HBM, warps per block) for cfg's precision form on this graph, `trials` runs each after a
+ * warm-up, and keeps the fastest on the handle for later runs of that form.  Scores are identical
+ * under every layout.  *layout (may be NULL) receives the choice: 0x100 bit = shared memory, low
+ * byte = warps per block.  The reference has no counterpart (its OpenMP loop has one layout). */
+tgtp_status tgtp_graph_tune(tgtp_graph* g, const tgtp_config* cfg, float* device_scores,
+                            int32_t trials, int32_t* layout);
+
+/* ---- batched tgtp ----------------------------------------------------------------------------- */
+/* Many tgtp() runs (src/aesc.h:120-127 each: its own graph, epsilon, omega, gamma and precision
+ * form) replayed as one CUDA graph.  Creation runs each configuration once (sizing its buffers;
+ * with tune_trials > 0 also tgtp_graph_tune), then captures all runs as parallel branches, one per
+ * graph; every graph may appear once.  Scores go to the caller-owned device buffers given here
+ * (m float32 each) on every tgtp_batch_run.  While the batch lives, its graphs keep their buffers:
+ * tgtp_eigens_upload, tgtp_graph_free and runs that would need larger buffers are refused. */
+typedef struct tgtp_batch tgtp_batch;
+tgtp_status tgtp_batch_create(tgtp_graph* const* graphs, const tgtp_config* configs,
+                              float* const* device_scores, uint32_t count, int32_t tune_trials,
+                              tgtp_batch** out);
+/* One cudaGraphLaunch on cuda_stream (NULL: the batch's own stream); asynchronous. */
+tgtp_status tgtp_batch_run(tgtp_batch* b, void* cuda_stream);
+/* Waits for the last tgtp_batch_run and reports a device time-out or walk-count error of any run;
+ * afterwards tgtp_last_run_stats of each graph describes its run in the batch. */
+tgtp_status tgtp_batch_wait(tgtp_batch* b);
+tgtp_status tgtp_batch_free(tgtp_batch* b);
+
 /* ---- SABA walk counter ---------------------------------------------------------------------- */
 /* n_walks walks of `depth` hops from every vertex with nonzero degree; counters[v] = visits of v
  * (start vertex excluded).  host_counters (n uint32) may be NULL.  Synchronous.

@@ -79,6 +79,12 @@ SIGNATURES = {
     "saba_count_device": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _vp]),
     "saba_count_static": (C.c_int, [_vp, _vp, _u64, C.c_uint32, C.c_uint32, _vp,
                                     C.POINTER(SabaResult)]),
+    "tgtp_graph_tune": (C.c_int, [_vp, C.POINTER(Config), _vp, C.c_int32, C.POINTER(C.c_int32)]),
+    "tgtp_batch_create": (C.c_int, [C.POINTER(_vp), C.POINTER(Config), C.POINTER(_vp), C.c_uint32,
+                                    C.c_int32, C.POINTER(_vp)]),
+    "tgtp_batch_run": (C.c_int, [_vp, _vp]),
+    "tgtp_batch_wait": (C.c_int, [_vp]),
+    "tgtp_batch_free": (C.c_int, [_vp]),
     "tgtp_release_cached_memory": (C.c_int, []),
     "tgtp_graph_set_profiling": (C.c_int, [_vp, C.c_int]),
     "tgtp_graph_kernel_stats": (C.c_int, [_vp, C.POINTER(KernelStat), C.c_int32,

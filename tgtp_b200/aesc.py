@@ -178,6 +178,47 @@ class AESC:
         check(lib().tgtp_last_taus(self.g.handle, ptr(out)))
         return out
 
+    def tune(self, device_ptr: int, trials: int = 3) -> int:
+        """Times the source-kernel layouts for this form on this graph and keeps the fastest
+        (tgtp_graph_tune); returns the layout code (0x100 = shared memory | warps per block)."""
+        cfg = self.config.to_c(self.g.n)
+        code = C.c_int32(0)
+        check(lib().tgtp_graph_tune(self.g.handle, C.byref(cfg), C.c_void_p(device_ptr), trials,
+                                    C.byref(code)))
+        return int(code.value)
+
+
+class Batch:
+    """Many tgtp() runs replayed as one CUDA graph (tgtp_batch_*).  `runs` is a list of
+    (AESC, device output pointer); every graph may appear once."""
+
+    def __init__(self, runs, tune_trials: int = 0):
+        self.runs = list(runs)
+        k = len(self.runs)
+        graphs = (C.c_void_p * k)(*[a.g.handle for a, _ in self.runs])
+        cfgs = (_lib.Config * k)(*[a.config.to_c(a.g.n) for a, _ in self.runs])
+        outs = (C.c_void_p * k)(*[C.c_void_p(p) for _, p in self.runs])
+        h = C.c_void_p()
+        check(lib().tgtp_batch_create(graphs, cfgs, outs, k, tune_trials, C.byref(h)))
+        self._h = h
+
+    def run(self, stream_ptr: int | None = None) -> None:
+        check(lib().tgtp_batch_run(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def wait(self) -> None:
+        check(lib().tgtp_batch_wait(self._h))
+
+    def free(self) -> None:
+        if self._h is not None:
+            check(lib().tgtp_batch_free(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
 
 def saba_count(g: AESCGraph, depth: int, n_walks: int, counters: bool = True):
     """(counters uint32[n] | None, visit_count, checksum, fallback_bouquets)."""

@@ -27,6 +27,10 @@
 #include <string>
 #include <type_traits>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -54,8 +58,18 @@ enum StatIdx {
 // warps of a launch do not all meet on one address; the host adds the copies up.
 constexpr int kStStripes = 32;
 
-// The run's work words ([0] next list entry, [1] error flags, [2] list length) sit behind the
-// striped counters in the same buffer.
+// Forms with their own tuned source-kernel layout on a handle: FP32, FP64, MIXED over F32 rows,
+// MIXED over BF16 rows.  A layout is (kLayoutSmem if the residual vectors live in shared memory) |
+// warps per block; 0 = the default rule.
+constexpr uint16_t kLayoutSmem = 0x100;
+inline int form_key(const tgtp_config& cfg) {
+    if (cfg.precision == TGTP_PRECISION_FP32) return 0;
+    if (cfg.precision == TGTP_PRECISION_FP64) return 1;
+    return cfg.vec_dtype == TGTP_VEC_BF16 ? 3 : 2;
+}
+
+// The run's work words ([0] next list entry, [1] error flags, [2] list length, [3] unused) sit
+// behind the striped counters in the same buffer, and the per-row marks behind them.
 inline unsigned* run_work(tgtp_graph* g) {
     return reinterpret_cast<unsigned*>(g->stats.as<unsigned char>() +
                                        sizeof(unsigned long long) * kStCount * kStStripes);
@@ -1723,6 +1737,16 @@ uint64_t deadline_from_env() {
     return uint64_t(s * 1e9);
 }
 
+// Buffer growth of a run.  A graph captured in a live batch must keep every buffer the batch's
+// CUDA graph points at, so a run on it that would need a larger buffer is refused.
+void grow(tgtp_graph* g, DeviceBuffer& b, size_t want) {
+    if (g->batch_refs > 0 && (!b.ptr || b.bytes < want))
+        fail(TGTP_ERR_INVALID_ARGUMENT,
+             "this graph belongs to a live batch and the run needs larger buffers than the batch's; "
+             "free the batch first");
+    b.reserve(want);
+}
+
 // Weight tables of the split tau kernel for the configured omega, cached on the graph: row 0 =
 // 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) from the same FP64 power chain as the
 // parity forms' eigen_t_1 table, zero at the indices the reference leaves out (0 and omega - 1)
@@ -1732,6 +1756,9 @@ uint32_t split_pad(uint32_t omega) { return (omega + 63u) & ~63u; }
 
 void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
     if (g->split_omega == omega && g->wtab32.ptr && g->wtab64.ptr) return;
+    if (g->batch_refs > 0)
+        fail(TGTP_ERR_INVALID_ARGUMENT,
+             "this graph belongs to a live batch built for another omega; free the batch first");
     const uint32_t rows = 1 + kTauTableRows, wpad = split_pad(omega);
     std::vector<double> t(size_t(rows) * wpad, 0.0);
     for (uint32_t i = 1; i + 1 < omega; ++i) {
@@ -1756,25 +1783,15 @@ void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
     g->split_omega = omega;
 }
 
-// Row marks of this run: a fresh epoch per run, the marks zeroed when the buffers are first made
-// (and when the epoch counter wraps).
+// Row marks of this run: they sit behind the work words in the counter buffer, so the run's one
+// zeroing clears them too (a captured run replays correctly), and a marked row holds 1.
 RowMarks begin_row_marks(tgtp_graph* g) {
-    const size_t bytes = sizeof(uint32_t) * (g->n + 1);
-    if (!g->row_mark.ptr || g->row_mark.bytes < bytes) {
-        g->row_mark.reserve(bytes);
-        g->row_list.reserve(bytes);
-        TGTP_CUDA(cudaMemsetAsync(g->row_mark.ptr, 0, bytes, g->stream));
-        g->row_epoch = 0;
-    }
-    if (++g->row_epoch == 0) {
-        TGTP_CUDA(cudaMemsetAsync(g->row_mark.ptr, 0, bytes, g->stream));
-        g->row_epoch = 1;
-    }
+    grow(g, g->row_list, sizeof(uint32_t) * (g->n + 1));
     RowMarks rm;
-    rm.mark = g->row_mark.as<uint32_t>();
+    rm.mark = run_work(g) + 4;
     rm.list = g->row_list.as<uint32_t>();
     rm.len = run_work(g) + 2;
-    rm.epoch = g->row_epoch;
+    rm.epoch = 1;
     return rm;
 }
 
@@ -1804,6 +1821,28 @@ void launch(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, 
     TGTP_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
 }
 
+// Resident blocks per SM of a kernel at a block size and dynamic shared memory, cached; the kernel's
+// dynamic shared-memory limit is raised to the largest size asked for so far.
+int blocks_per_sm(const void* kern, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, size_t, int>, int> cache;
+    static std::map<const void*, size_t> limit;
+    int dev = 0;
+    TGTP_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_tuple(kern, threads, smem, dev);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    if (smem > limit[kern]) {
+        TGTP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        limit[kern] = smem;
+    }
+    int per_sm = 0;
+    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    cache[key] = per_sm;
+    return per_sm;
+}
+
 // One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
 // JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
 template <class Real, class Acc, bool JACOBI, class Vec>
@@ -1820,14 +1859,15 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     c.b2 = std::log(double(1.0) / std::fabs(l2));
     const double logmd = std::log(double(m) / cfg.delta);
 
-    g->taus.reserve(sizeof(int) * (m + 1));
-    g->preds.reserve(sizeof(Acc) * (m + 1));
-    // one zeroing for the striped counters and the work words behind them
+    grow(g, g->taus, sizeof(int) * (m + 1));
+    grow(g, g->preds, sizeof(Acc) * (m + 1));
+    // one zeroing for the striped counters, the work words and the row marks behind them
     const size_t stat_bytes = sizeof(unsigned long long) * kStCount * kStStripes;
-    g->stats.reserve(stat_bytes + sizeof(unsigned) * 4);
+    const size_t zero_bytes = stat_bytes + sizeof(unsigned) * (4 + n + 1);
+    grow(g, g->stats, zero_bytes);
     auto* stats = g->stats.as<unsigned long long>();
     auto* work = run_work(g);
-    TGTP_CUDA(cudaMemsetAsync(stats, 0, stat_bytes + sizeof(unsigned) * 4, s));
+    TGTP_CUDA(cudaMemsetAsync(stats, 0, zero_bytes, s));
 
     const RowMarks rm = begin_row_marks(g);
     if constexpr (JACOBI || std::is_same<Real, double>::value) {
@@ -1841,11 +1881,10 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
                                                              : (const Part*)g->wtab32.ptr;
         const uint32_t wpad = split_pad(omega);
         const size_t ssmem = 2 * sizeof(Part) * wpad;
-        int per_sm = 0;
-        TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tau_sums_kernel<Vec>, 256,
-                                                                ssmem));
+        const int per_sm =
+            blocks_per_sm(reinterpret_cast<const void*>(tau_sums_kernel<Vec>), 256, ssmem);
         if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel");
-        g->tau_sums.reserve(sizeof(double2) * (g->num_forward + 1));
+        grow(g, g->tau_sums, sizeof(double2) * (g->num_forward + 1));
         const uint64_t need = (g->num_forward + 63) / 64;  // 64 edges per block and step
         const unsigned blocks = unsigned(std::max<uint64_t>(
             1, std::min<uint64_t>(need, uint64_t(g->num_sms) * per_sm)));
@@ -1873,11 +1912,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
                                 size_t(kTauThreads / 32) * 4 * 32 * (128 / sizeof(Real) + 1) * sizeof(Real);
         if (tau_smem > size_t(227) * 1024)
             fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel tile");
-        TGTP_CUDA(cudaFuncSetAttribute(tau_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(tau_smem)));
-        int tau_per_sm = 0;
-        TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tau_per_sm, tau_kernel<Real>,
-                                                                kTauThreads, tau_smem));
+        const int tau_per_sm =
+            blocks_per_sm(reinterpret_cast<const void*>(tau_kernel<Real>), kTauThreads, tau_smem);
         if (tau_per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel tile");
         const uint64_t groups = (g->num_forward + 31) / 32;
         const uint64_t tau_blocks = std::max<uint64_t>(1, std::min<uint64_t>(
@@ -1891,25 +1927,35 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         TGTP_LAUNCH_CHECK("tau_kernel");
     }
 
-    // source kernel.  Shared-memory tier: one warp per block, each with its residual vector and
-    // flags in shared memory (one-warp blocks give the finest occupancy steps).  Global tier
-    // (large n): 4 warps per block, vectors in HBM.  TGTP_PVEC_TIER=smem|global overrides.
+    // source kernel.  Shared-memory tier: each warp's residual vector and flags in shared memory.
+    // Global tier (large n): vectors in HBM.  The layout (tier, warps per block) comes from the
+    // handle's tuned choice for this form, else from the default rule (shared memory with one-warp
+    // blocks while a warp's copy fits in 112 KB, else HBM with four warps per block);
+    // TGTP_PVEC_TIER=smem|global overrides the tier of the default rule.
     const size_t pv_bytes = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
     const size_t vis_bytes = (size_t(n) + 15) & ~size_t(15);
     const size_t per_warp = pv_bytes + vis_bytes + kAccBytes;
-    bool use_smem = per_warp <= size_t(112) * 1024;
-    if (const char* t = std::getenv("TGTP_PVEC_TIER")) {
-        if (std::string(t) == "global") use_smem = false;
-        else if (std::string(t) == "smem" && per_warp <= size_t(227) * 1024) use_smem = true;
+    const int key = form_key(cfg);
+    bool use_smem;
+    int wpb;
+    if (g->src_layout[key]) {
+        use_smem = (g->src_layout[key] & kLayoutSmem) != 0;
+        wpb = g->src_layout[key] & 0xff;
+    } else {
+        use_smem = per_warp <= size_t(112) * 1024;
+        if (const char* t = std::getenv("TGTP_PVEC_TIER")) {
+            if (std::string(t) == "global") use_smem = false;
+            else if (std::string(t) == "smem" && per_warp <= size_t(227) * 1024) use_smem = true;
+        }
+        wpb = use_smem ? 1 : 4;
     }
-    const int wpb = use_smem ? 1 : 4;
+    if (use_smem && per_warp * wpb > size_t(227) * 1024)
+        fail(TGTP_ERR_UNSUPPORTED, "source layout does not fit in shared memory");
     const int threads = wpb * 32;
     const size_t smem = use_smem ? per_warp * wpb : size_t(wpb) * kAccBytes;
     auto kern = use_smem ? source_kernel<Real, Acc, true, JACOBI>
                          : source_kernel<Real, Acc, false, JACOBI>;
-    TGTP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    int per_sm = 0;
-    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    const int per_sm = blocks_per_sm(reinterpret_cast<const void*>(kern), threads, smem);
     if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "source kernel does not fit on an SM");
     uint64_t blocks = uint64_t(g->num_sms) * per_sm;
     blocks = std::min<uint64_t>(blocks, (n + wpb - 1) / wpb);
@@ -1921,7 +1967,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(Real)) : 0;
     const size_t pvg_bytes = use_smem ? 0 : align(warps * size_t(n) * sizeof(Real));
     const size_t visg_bytes = use_smem ? 0 : align(warps * vis_bytes);
-    g->scratch.reserve(q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + 256);
+    grow(g, g->scratch, q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
     SourceParams<Real, Acc> p;
     p.idx = g->idx.as<uint32_t>();
@@ -2008,12 +2054,7 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
     g->have_run = true;
 }
 
-}  // namespace tgtp
-
-using namespace tgtp;
-
-namespace {
-void finish_run(tgtp_graph* g) {
+void aesc_check_flags(tgtp_graph* g) {
     unsigned flags[2];
     TGTP_CUDA(cudaMemcpyAsync(flags, run_work(g), sizeof(flags), cudaMemcpyDeviceToHost, g->stream));
     TGTP_CUDA(cudaStreamSynchronize(g->stream));
@@ -2022,6 +2063,66 @@ void finish_run(tgtp_graph* g) {
     if (flags[1] & kErrWalkCount)
         fail(TGTP_ERR_UNSUPPORTED, "a walk count exceeds the 32-bit walk grid");
 }
+
+int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials) {
+    const int key = form_key(cfg);
+    const size_t rs = cfg.precision == TGTP_PRECISION_FP64 ? 8 : 4;
+    const size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
+    std::vector<uint16_t> cand;
+    for (int w : {1, 2})
+        if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(kLayoutSmem | w));
+    for (int w : {1, 2, 4}) cand.push_back(uint16_t(w));
+    cudaEvent_t e0, e1;
+    TGTP_CUDA(cudaEventCreate(&e0));
+    TGTP_CUDA(cudaEventCreate(&e1));
+    const bool prof = g->prof.enabled;
+    g->prof.enabled = false;
+    float best = 0;
+    uint16_t pick = 0;
+    try {
+        for (uint16_t c : cand) {
+            g->src_layout[key] = c;
+            try {
+                aesc_run(g, cfg, device_scores);  // warm-up (and scratch for this layout)
+            } catch (const Error&) {
+                continue;  // the layout does not fit this graph
+            }
+            float t = 0;
+            for (int i = 0; i < std::max(trials, 1); ++i) {
+                TGTP_CUDA(cudaEventRecord(e0, g->stream));
+                aesc_run(g, cfg, device_scores);
+                TGTP_CUDA(cudaEventRecord(e1, g->stream));
+                TGTP_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                TGTP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                t = i == 0 ? ms : std::min(t, ms);
+            }
+            if (!pick || t < best) {
+                best = t;
+                pick = c;
+            }
+        }
+    } catch (...) {
+        g->src_layout[key] = 0;
+        g->prof.enabled = prof;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    g->src_layout[key] = pick;
+    g->prof.enabled = prof;
+    TGTP_CUDA(cudaEventDestroy(e0));
+    TGTP_CUDA(cudaEventDestroy(e1));
+    if (!pick) fail(TGTP_ERR_UNSUPPORTED, "no source-kernel layout fits this graph");
+    return pick;
+}
+
+}  // namespace tgtp
+
+using namespace tgtp;
+
+namespace {
+void finish_run(tgtp_graph* g) { aesc_check_flags(g); }
 }  // namespace
 
 extern "C" {

@@ -436,7 +436,11 @@ tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t
 }
 
 tgtp_status tgtp_graph_free(tgtp_graph* g) {
-    return guarded([&] { delete g; });
+    return guarded([&] {
+        if (g && g->batch_refs > 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "this graph belongs to a live batch; free the batch first");
+        delete g;
+    });
 }
 
 tgtp_status tgtp_graph_set_stream(tgtp_graph* g, void* cuda_stream) {
@@ -461,6 +465,8 @@ tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* 
                                uint32_t omega, int32_t dtype, int32_t store_dtype) {
     return guarded([&] {
         if (!g || !values || !vectors) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
+        if (g->batch_refs > 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "this graph belongs to a live batch; free the batch first");
         if (omega < 2 || omega > g->n)
             fail(TGTP_ERR_INVALID_ARGUMENT, "omega must be between 2 and vertex count");
         if (dtype != TGTP_VEC_F32 && dtype != TGTP_VEC_F64)

@@ -168,8 +168,9 @@ struct tgtp_graph {
     tgtp::DeviceBuffer onep, onem, etab, etab_f;
     tgtp::DeviceBuffer wtab32, wtab64;  // weights of the split tau kernel for split_omega
     uint32_t split_omega = 0;
-    tgtp::DeviceBuffer row_mark, row_list;  // rows with a slot of tau > 1 (this run's epoch)
-    uint32_t row_epoch = 0;
+    tgtp::DeviceBuffer row_list;  // rows with a slot of tau > 1 (their marks follow the counters)
+    uint16_t src_layout[4] = {0, 0, 0, 0};  // tuned source-kernel layout per form (0 = default)
+    int batch_refs = 0;  // live batches whose CUDA graph points at this handle's buffers
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
@@ -190,5 +191,10 @@ namespace tgtp {
 void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_counters);
 void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* host_sums3);
 void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores);
+// Times the candidate source-kernel layouts of cfg's form on this graph (trials runs each, after
+// one warm-up) and keeps the fastest on the handle.  Returns the chosen layout code.
+int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials);
+// Error flags of the handle's last run as a failure (synchronises the handle's stream).
+void aesc_check_flags(tgtp_graph* g);
 void graph_prepare(tgtp_graph* g);
 }  // namespace tgtp
