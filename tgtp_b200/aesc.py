@@ -22,7 +22,7 @@ from . import _lib
 from ._lib import (PRECISION_FP32, PRECISION_FP64, PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64,
                    TgtpError, check, lib, ptr)
 
-__all__ = ["AESCGraph", "AESCConfig", "AESC", "saba_count", "load_graph_txt", "load_eigens_txt",
+__all__ = ["AESCGraph", "AESCConfig", "AESC", "Batch", "saba_count", "load_graph_txt", "load_eigens_txt",
            "TgtpError", "PRECISION_FP32", "PRECISION_FP64", "PRECISION_MIXED", "VEC_F32", "VEC_F64",
            "VEC_BF16"]
 

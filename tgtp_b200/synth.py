@@ -145,3 +145,28 @@ def config1_graph(seed: int = 1) -> EdgeList:
 def config3_graph(seed: int = 1) -> EdgeList:
     """R-MAT scale 18, edge factor 16, a=0.57, b=c=0.19: the SABA throughput workload."""
     return rmat(18, 16, 0.57, 0.19, 0.19, seed)
+
+
+def config5_graphs(seed: int = 5, count: int = 64):
+    """The batched workload: `count` graphs of uneven size, n log-uniform in [1,000, 200,000], a
+    third each Chung-Lu (exponent 2.1-2.8), R-MAT (a=0.57, b=c=0.19) and 2-D grid with random
+    chords, average degree 8-40, each with its own epsilon from {0.05, 0.01, 0.005}.  Returns a
+    list of (EdgeList, epsilon); every graph has its own seed derived from `seed`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(1000), np.log(200000)))))
+        deg = float(rng.uniform(8, 40))
+        eps = float(rng.choice([0.05, 0.01, 0.005]))
+        gseed = int(rng.integers(1, 2**31 - 1))
+        kind = i % 3
+        if kind == 0:
+            g = chung_lu(n, int(n * deg / 2), float(rng.uniform(2.1, 2.8)), gseed)
+        elif kind == 1:
+            scale = max(10, int(round(np.log2(n))))
+            g = rmat(scale, max(4, int(round(deg / 2))), 0.57, 0.19, 0.19, gseed)
+        else:
+            rows = max(2, int(round(np.sqrt(n))))
+            g = grid_chords(rows, max(2, n // rows), deg, gseed)
+        out.append((g, eps))
+    return out
