@@ -29,8 +29,13 @@ def _rev(idx, adj):
     return order[np.searchsorted(key[order], adj.astype(np.int64) * len(idx) + rows)]
 
 
+@pytest.mark.parametrize("block", ["0", "1"])
 @pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
-def test_mixed_deterministic_symmetric_and_as_accurate_as_fp64(manifest, cuda_device, name):
+def test_mixed_deterministic_symmetric_and_as_accurate_as_fp64(manifest, cuda_device, name, block,
+                                                              monkeypatch):
+    """block = 1 forces the multi-source push (push_block_kernel + source_kernel in PrePush mode)
+    that large graphs take; 0 the per-warp push."""
+    monkeypatch.setenv("TGTP_MIXED_BLOCK", block)
     from oracle import exact_sc
     from tgtp_b200.aesc import (AESC, AESCConfig, PRECISION_FP64, PRECISION_MIXED, VEC_BF16,
                                 VEC_F32)

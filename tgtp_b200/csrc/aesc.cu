@@ -28,6 +28,8 @@
 #include <type_traits>
 
 #include <map>
+
+#include <cub/device/device_radix_sort.cuh>
 #include <mutex>
 #include <tuple>
 
@@ -688,6 +690,13 @@ struct WalkItem {
     unsigned long long nr;
 };
 
+// Outcome of the push of one listed source in push_block_kernel.
+struct PrePush {
+    int ell;           // rounds pushed
+    float gmax, gmin;  // residual max / min over the final frontier (gmin before the |q| < n rule)
+    uint32_t support;  // size of the final frontier
+};
+
 template <class Real, class Acc>
 struct SourceParams {
     const uint32_t* idx;
@@ -712,6 +721,14 @@ struct SourceParams {
     unsigned long long* stats;
     const uint2* adjd;    // (neighbour, neighbour degree) per slot
     uint64_t budget_ns;   // device time budget; past it every warp stops and flags a timeout
+    unsigned* claim;      // the claim counter of this launch
+    uint32_t list_base;   // this launch runs list entries [list_base, list_base + list_cap)
+    uint32_t list_cap;
+    // PrePush mode (mixed form, large graphs): the push ran in push_block_kernel; entry k's final
+    // residual vector is column (k - list_base) % S of its CTA's block
+    const PrePush* pre;
+    const float* pre_cols;
+    const uint32_t* pre_final;
 };
 
 template <class Real>
@@ -874,6 +891,261 @@ __device__ __forceinline__ void seg_maxmin(uint32_t seg, Real& mx, Real& mn) {
     }
 }
 
+// ---- stage 2a (mixed form, large graphs): multi-source Jacobi push as a pull product -----------
+// In the mixed form a push round drains the whole frontier at once (Jacobi), so a round is exactly
+// r <- D^-1 A r: with r supported on the frontier q, every vertex u receives the residuals of its
+// frontier neighbours divided by deg(u), and the frontier's own residuals are pushed out.  For
+// graphs whose residual vector does not fit in shared memory, each CTA takes S = 32 listed sources
+// at a time and keeps their residual vectors as the columns of an n x S row-major block in HBM; a
+// round is one pass over the CSR in which warp w pulls rows u = w, w + 32, ...: lane j adds the
+// column-j entries of u's neighbours in CSR order (one coalesced 128-byte row read per neighbour)
+// and divides by deg(u).  The same pass accumulates each column's frontier statistics (degree sum,
+// max, min, size of the support), so the stop test of src/aesc.h:483-502 needs no further pass.
+// Columns whose source has stopped are carried over unchanged, so when the last one stops every
+// column holds its source's final residual vector; the edge bound, chi and walks of those sources
+// then run in source_kernel (PrePush mode), which copies the column into its own residual vector.
+constexpr int kBlockCols = 32;
+
+
+struct PushBlockParams {
+    const uint32_t* idx;
+    const uint32_t* adj;
+    const uint32_t* deg;
+    const uint2* adjd;
+    uint32_t n;
+    const int* taus;
+    double* preds;
+    unsigned* work;        // [1] error flags, [2] list length
+    const uint32_t* rows;  // the list of sources
+    uint32_t base;         // first list entry of this wave
+    double eps, logmd;
+    float* cols;           // per CTA: two n x S blocks
+    uint32_t* final_buf;   // per CTA: the block that holds the final columns
+    PrePush* pre;          // per list entry
+    unsigned long long* stats;
+    uint64_t budget_ns;
+};
+
+__global__ void __launch_bounds__(1024, 1)
+push_block_kernel(PushBlockParams p) {
+    constexpr int S = kBlockCols;
+    __shared__ uint32_t s_src[S], s_rb[S], s_ds[S], s_support[S], s_ell[S];
+    __shared__ unsigned long long s_picost[S];
+    __shared__ unsigned s_max[S], s_min[S];  // float bits of non-negative residuals
+    __shared__ int s_active[S];
+    __shared__ int s_any;
+    pdl_launch_dependents();
+    pdl_wait();  // the list, and the previous wave's readers of these blocks
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const uint32_t n = p.n;
+    const unsigned len = p.work[2];
+    const uint64_t first = uint64_t(p.base) + uint64_t(blockIdx.x) * S;
+    if (first >= len) return;
+    const uint32_t cnt = uint32_t(min(uint64_t(S), len - first));
+    float* A = p.cols + size_t(blockIdx.x) * 2 * size_t(n) * S;
+    float* B = A + size_t(n) * S;
+    const uint64_t deadline = globaltimer_ns() + p.budget_ns;
+    unsigned long long st_pv = 0, st_tr = 0, st_rounds = 0;
+
+    // round 1 in closed form: the frontier {src} pushes 1 / deg(u) to every neighbour u
+    for (size_t i = threadIdx.x; i < size_t(n) * S / 4; i += blockDim.x)
+        reinterpret_cast<float4*>(A)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (threadIdx.x < S) {
+        const uint32_t j = threadIdx.x;
+        s_active[j] = j < cnt;
+        s_src[j] = j < cnt ? __ldg(p.rows + first + j) : 0;
+        s_picost[j] = 0;
+        s_max[j] = 0;
+        s_min[j] = __float_as_uint(1.f);
+        s_ell[j] = 1;
+    }
+    __syncthreads();
+    if (warp < cnt) {
+        const uint32_t j = warp, src = s_src[j];
+        const uint32_t rb = __ldg(p.idx + src), dsi = __ldg(p.idx + src + 1) - rb;
+        const float ds = float(dsi);
+        const double pinit = __ddiv_rn(1.0, double(ds));
+        unsigned long long pc = 0;
+        float mx = 0.f, mn = 1.f;
+        for (uint32_t o = lane; o < dsi; o += 32) {
+            const uint2 a = __ldg(p.adjd + rb + o);
+            const float pu = __fdiv_rn(1.f, float(a.y));
+            A[size_t(a.x) * S + j] = pu;
+            pc += a.y;
+            mx = fmaxf(mx, pu);
+            mn = fminf(mn, pu);
+            p.preds[rb + o] = row_update<float, double>(pinit, 0.f, pu, ds);
+        }
+        pc = warp_sum_u64(pc);
+        mx = warp_max(mx);
+        mn = warp_min(mn);
+        if (lane == 0) {
+            s_rb[j] = rb;
+            s_ds[j] = dsi;
+            s_picost[j] = pc;
+            s_max[j] = __float_as_uint(mx);
+            s_min[j] = __float_as_uint(mn);
+            s_support[j] = dsi;
+        }
+        st_pv += lane == 0 ? 1 : 0;
+        st_tr += lane == 0 ? dsi : 0;
+    }
+    __syncthreads();
+    float* cur = A;
+    float* nxt = B;
+    uint32_t fin = 0;
+    while (true) {
+        // ---- stop test of every running source (one warp per source) ----
+        if (threadIdx.x == 0) s_any = 0;
+        __syncthreads();
+        if (warp < cnt && s_active[warp]) {
+            const uint32_t j = warp, rb = s_rb[j], dsi = s_ds[j];
+            const int ell = int(s_ell[j]);
+            const float gmax = __uint_as_float(s_max[j]);
+            const float gmin = s_support[j] < n ? 0.f : __uint_as_float(s_min[j]);
+            const double dse0 = __dmul_rn(double(float(dsi)), p.eps);
+            const double dse2 = __dmul_rn(dse0, dse0);
+            double rw = 0;
+            for (uint32_t c = 0; c < dsi; c += 32) {
+                const uint32_t o = c + lane;
+                const int rest = o < dsi ? __ldg(p.taus + rb + o) - ell : 0;
+                double nrd = 0;
+                const bool has = rest > 0;
+                if (has) {
+                    const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
+                                                 __dsub_rn(double(gmax), double(gmin)));
+                    const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
+                    nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
+                }
+                unsigned hb = __ballot_sync(kFullMask, has);
+                while (hb) {  // rwcost += nr in slot order
+                    const int l = __ffs(hb) - 1;
+                    hb &= hb - 1;
+                    rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
+                }
+            }
+            const bool stop = double(s_picost[j]) >= __dmul_rn(25.0, rw);
+            const bool late = globaltimer_ns() > deadline;
+            if (lane == 0) {
+                if (stop || late) {
+                    s_active[j] = 0;
+                    PrePush r;
+                    r.ell = ell;
+                    r.gmax = gmax;
+                    r.gmin = __uint_as_float(s_min[j]);
+                    r.support = s_support[j];
+                    p.pre[first + j] = r;
+                    st_rounds += uint64_t(ell);
+                    if (late && !stop) atomicOr(p.work + 1, kErrDeadline);
+                } else {
+                    s_any = 1;
+                    st_pv += s_support[j];
+                    st_tr += s_picost[j];
+                }
+            }
+        }
+        __syncthreads();
+        if (!s_any) break;
+        // ---- one Jacobi round for the running columns; stopped columns are carried over ----
+        if (threadIdx.x < S) {
+            s_picost[threadIdx.x] = 0;
+            s_max[threadIdx.x] = 0;
+            s_min[threadIdx.x] = __float_as_uint(1.f);
+            s_support[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        const bool run = lane < cnt && s_active[lane];
+        unsigned long long pc = 0;
+        uint32_t sup = 0;
+        float mx = 0.f, mn = 1.f;
+        for (uint32_t u = warp; u < n; u += nwarp) {
+            const uint32_t ub = __ldg(p.idx + u), ud = __ldg(p.idx + u + 1) - ub;
+            float acc = 0.f;
+            for (uint32_t c = 0; c < ud; c += 32) {
+                const uint32_t nb = c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u;
+                const uint32_t k = min(32u, ud - c);
+                uint32_t t = 0;
+                for (; t + 4 <= k; t += 4) {
+                    const float x0 = cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane];
+                    const float x1 = cur[size_t(__shfl_sync(kFullMask, nb, t + 1)) * S + lane];
+                    const float x2 = cur[size_t(__shfl_sync(kFullMask, nb, t + 2)) * S + lane];
+                    const float x3 = cur[size_t(__shfl_sync(kFullMask, nb, t + 3)) * S + lane];
+                    acc = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(acc, x0), x1), x2), x3);
+                }
+                for (; t < k; ++t) acc = __fadd_rn(acc, cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane]);
+            }
+            float r = cur[size_t(u) * S + lane];
+            if (run) {
+                r = acc > 0.f ? __fdiv_rn(acc, float(ud)) : 0.f;
+                if (r > 0.f) {
+                    pc += ud;
+                    ++sup;
+                    mx = fmaxf(mx, r);
+                    mn = fminf(mn, r);
+                }
+            }
+            nxt[size_t(u) * S + lane] = r;
+        }
+        if (run) {
+            atomicAdd(s_picost + lane, pc);
+            atomicAdd(s_support + lane, sup);
+            atomicMax(s_max + lane, __float_as_uint(mx));
+            atomicMin(s_min + lane, __float_as_uint(mn));
+        }
+        __syncthreads();
+        // ---- preds[row] += (r[src] - r[t]) / ds for every slot of each running source ----
+        if (warp < cnt && s_active[warp]) {
+            const uint32_t j = warp, src = s_src[j], rb = s_rb[j], dsi = s_ds[j];
+            const float ds = float(dsi);
+            const float ps = nxt[size_t(src) * S + j];
+            for (uint32_t o = lane; o < dsi; o += 32) {
+                const uint32_t w = __ldg(p.adj + rb + o);
+                p.preds[rb + o] = row_update<float, double>(p.preds[rb + o], ps,
+                                                            nxt[size_t(w) * S + j], ds);
+            }
+            if (lane == 0) ++s_ell[j];
+        }
+        __syncthreads();
+        float* t = cur;
+        cur = nxt;
+        nxt = t;
+        fin ^= 1u;
+    }
+    if (threadIdx.x == 0) p.final_buf[blockIdx.x] = fin;
+    st_pv = warp_sum_u64(st_pv);
+    st_tr = warp_sum_u64(st_tr);
+    st_rounds = warp_sum_u64(st_rounds);
+    if (lane == 0) {
+        stat_add(p.stats, kStPushRounds, st_rounds);
+        stat_add(p.stats, kStPushVertices, st_pv);
+        stat_add(p.stats, kStPushTraversals, st_tr);
+    }
+}
+
+// Sort key of each row for the multi-source push: the row's largest tau if it is listed, else 0.
+// A source stops pushing once ell reaches that tau (rwcost = 0 then), so CTAs whose 32 sources
+// share a tau bound push for about the same number of rounds.
+__global__ void row_key_kernel(const uint32_t* __restrict__ idx, const int* __restrict__ taus,
+                               const uint32_t* __restrict__ mark, uint32_t n,
+                               uint32_t* __restrict__ key, uint32_t* __restrict__ ids) {
+    pdl_wait();  // taus and marks of the tau kernels
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n;
+         v += (gridDim.x * blockDim.x) >> 5) {
+        int t = 0;
+        if (mark[v]) {
+            const uint32_t b = __ldg(idx + v), e = __ldg(idx + v + 1);
+            for (uint32_t o = b + lane; o < e; o += 32) t = max(t, __ldg(taus + o));
+#pragma unroll
+            for (int o = 16; o; o >>= 1) t = max(t, __shfl_xor_sync(kFullMask, t, o));
+        }
+        if (lane == 0) {
+            key[v] = uint32_t(t);
+            ids[v] = v;
+        }
+    }
+}
+
 template <class Real, class Acc, bool SMEM, bool JACOBI>
 __global__ void __launch_bounds__(kSrcMaxThreads)
 source_kernel(SourceParams<Real, Acc> p) {
@@ -922,7 +1194,8 @@ source_kernel(SourceParams<Real, Acc> p) {
 
     pdl_launch_dependents();
     pdl_wait();  // taus, row list and its length from the tau kernels
-    const unsigned nrows = p.work[2];  // final: the tau kernel that appends to the list has ended
+    const unsigned total = p.work[2];  // final: the tau kernel that appends to the list has ended
+    const unsigned nrows = total > p.list_base ? min(total - p.list_base, p.list_cap) : 0u;
     // list entry gw first, then entries past the grid's warps claimed one at a time (warps past
     // the list's end leave without touching the counter)
     const uint64_t nwarps = uint64_t(gridDim.x) * wpb;
@@ -931,7 +1204,7 @@ source_kernel(SourceParams<Real, Acc> p) {
         uint64_t k = gw;
         if (!first_claim) {
             unsigned c = 0;
-            if (lane == 0) c = atomicAdd(p.work, 1u);
+            if (lane == 0) c = atomicAdd(p.claim, 1u);
             k = nwarps + __shfl_sync(kFullMask, c, 0);
         }
         first_claim = false;
@@ -940,7 +1213,8 @@ source_kernel(SourceParams<Real, Acc> p) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);
             break;
         }
-        const uint32_t src = __ldg(p.rows + k);
+        const uint32_t entry = p.list_base + uint32_t(k);
+        const uint32_t src = __ldg(p.rows + entry);
         if (!cleared) {
             for (uint32_t i = lane; i < n; i += 32) {
                 pvec[i] = Real(0);
@@ -978,340 +1252,366 @@ source_kernel(SourceParams<Real, Acc> p) {
             }
         };
         lap(0);
-        // ---- round 1 in closed form (:457-503, first pass of the loop) ----
-        // The frontier is {src} with residual 1 (pvec[src] = 1.0, then zeroed as it is drained):
-        // every neighbour u is discovered in row order and receives 0 + 1/deg(u) = 1/deg(u), so
-        // the round's new frontier, residuals, degree sum, max / min and row update
-        // preds = 1/ds + (0 - 1/deg(u)) / ds follow from one pass over the row.  Neighbours are
-        // distinct (tgtp_run rejects repeated neighbours and self-loops).
-        pipelined<uint2>(dsi,
-            [&](uint32_t c, uint2* r) {
-#pragma unroll
-                for (int b = 0; b < kB; ++b) {
-                    const uint32_t o = c + 32 * b + lane;
-                    r[b] = o < dsi ? __ldg(p.adjd + rb + o) : make_uint2(NONE, 1u);
-                }
-            },
-            [&](uint32_t c, const uint2* r) {
-#pragma unroll
-                for (int b = 0; b < kB; ++b) {
-                    if (r[b].x == NONE) continue;
-                    const uint32_t o = c + 32 * b + lane;
-                    const Real pu = rdiv(Real(1), from_u64<Real>(r[b].y));
-                    pvec[r[b].x] = pu;
-                    qn[o] = r[b].x;
-                    pcost += r[b].y;
-                    mx = std_max(mx, pu);
-                    mn = std_min(mn, pu);
-                    p.preds[rb + o] = row_update<Real, Acc>(pinit, Real(0), pu, ds);
-                }
-            });
-        st_pv += 1;
-        st_tr += dsi;
-        qs = dsi;
-        ell = 1;
-        { uint32_t* tmp = q; q = qn; qn = tmp; }
-        __syncwarp();
-        lap(1);
-        while (true) {
-            // ---- the push/walk cost test (:483-502) ----
-            const double picost = double(warp_sum_u64(pcost));
-            gmax = warp_max(mx);
-            gmin = warp_min(mn);
-            gmin = qs < n ? Real(0) : gmin;
-            const double dse0 = __dmul_rn(double(ds), p.eps);
-            const double dse2 = __dmul_rn(dse0, dse0);
-            double rw = 0;
-            pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
-#pragma unroll
-                for (int b = 0; b < kB; ++b) {
-                    const uint32_t o = c + 32 * b + lane;
-                    const int rest = tv[b] - ell;
-                    double nrd = 0;
-                    const bool has = o < dsi && rest > 0;
-                    if (has) {
-                        const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
-                                                     __dsub_rn(double(gmax), double(gmin)));
-                        const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
-                        nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
-                    }
-                    unsigned hb = __ballot_sync(kFullMask, has);
-                    while (hb) {  // rwcost += nr in slot order
-                        const int l = __ffs(hb) - 1;
-                        hb &= hb - 1;
-                        rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
-                    }
-                }
-            });
-            lap(3);
-            if (picost >= __dmul_rn(25.0, rw)) break;
-            if (globaltimer_ns() > deadline) {
-                timed_out = true;
-                break;
+        if (p.pre) {
+            // The push ran in push_block_kernel: take the source's final residual vector from its
+            // column and rebuild the final frontier (the support) in vertex order.
+            const PrePush pr = p.pre[entry];
+            const uint32_t slot = entry - p.list_base;
+            const uint32_t cta = slot / kBlockCols, col = slot % kBlockCols;
+            const float* cb = p.pre_cols +
+                              (size_t(cta) * 2 + p.pre_final[cta]) * size_t(n) * kBlockCols + col;
+            uint32_t cq = 0;
+            for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+                const uint32_t i = i0 + lane;
+                const Real x = i < n ? Real(cb[size_t(i) * kBlockCols]) : Real(0);
+                if (i < n) pvec[i] = x;
+                const bool nz = x > Real(0);
+                const unsigned bal = __ballot_sync(kFullMask, nz);
+                if (nz) q[cq + __popc(bal & lt)] = i;
+                cq += __popc(bal);
             }
-            uint32_t qns = 0;
-            pcost = 0;
-            st_pv += qs;
-            if constexpr (!JACOBI) {
-            // ---- diffuse (:218-239) ----
-            // The frontier is drained in order, one vertex at a time; the lanes share the
-            // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
-            // touch distinct bytes and words).  Per batch of 32 frontier vertices the adjacency is
-            // cut into 32-slot chunks walked by a cursor; a chunk's (neighbour, degree) pairs are
-            // one coalesced 8-byte load per lane, issued kPushAhead chunks before use.  picost (the
-            // new frontier's degree sum) is summed on discovery.  Every vertex has at least one
-            // chunk: tgtp_run rejects isolated vertices.
-
-            for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
-                uint32_t myv = 0, myb = 0, myd = 0;
-                if (i0 + lane < qs) {
-                    myv = q[i0 + lane];
-                    myb = __ldg(idx + myv);
-                    myd = __ldg(idx + myv + 1) - myb;
+            __syncwarp();
+            qs = cq;
+            ell = pr.ell;
+            gmax = Real(pr.gmax);
+            gmin = qs < n ? Real(0) : Real(pr.gmin);
+            lap(1);
+        } else {
+            // ---- round 1 in closed form (:457-503, first pass of the loop) ----
+            // The frontier is {src} with residual 1 (pvec[src] = 1.0, then zeroed as it is drained):
+            // every neighbour u is discovered in row order and receives 0 + 1/deg(u) = 1/deg(u), so
+            // the round's new frontier, residuals, degree sum, max / min and row update
+            // preds = 1/ds + (0 - 1/deg(u)) / ds follow from one pass over the row.  Neighbours are
+            // distinct (tgtp_run rejects repeated neighbours and self-loops).
+            pipelined<uint2>(dsi,
+                [&](uint32_t c, uint2* r) {
+    #pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        const uint32_t o = c + 32 * b + lane;
+                        r[b] = o < dsi ? __ldg(p.adjd + rb + o) : make_uint2(NONE, 1u);
+                    }
+                },
+                [&](uint32_t c, const uint2* r) {
+    #pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        if (r[b].x == NONE) continue;
+                        const uint32_t o = c + 32 * b + lane;
+                        const Real pu = rdiv(Real(1), from_u64<Real>(r[b].y));
+                        pvec[r[b].x] = pu;
+                        qn[o] = r[b].x;
+                        pcost += r[b].y;
+                        mx = std_max(mx, pu);
+                        mn = std_min(mn, pu);
+                        p.preds[rb + o] = row_update<Real, Acc>(pinit, Real(0), pu, ds);
+                    }
+                });
+            st_pv += 1;
+            st_tr += dsi;
+            qs = dsi;
+            ell = 1;
+            { uint32_t* tmp = q; q = qn; qn = tmp; }
+            __syncwarp();
+            lap(1);
+            while (true) {
+                // ---- the push/walk cost test (:483-502) ----
+                const double picost = double(warp_sum_u64(pcost));
+                gmax = warp_max(mx);
+                gmin = warp_min(mn);
+                gmin = qs < n ? Real(0) : gmin;
+                const double dse0 = __dmul_rn(double(ds), p.eps);
+                const double dse2 = __dmul_rn(dse0, dse0);
+                double rw = 0;
+                pipelined<int>(dsi, load_tau, [&](uint32_t c, const int* tv) {
+    #pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        const uint32_t o = c + 32 * b + lane;
+                        const int rest = tv[b] - ell;
+                        double nrd = 0;
+                        const bool has = o < dsi && rest > 0;
+                        if (has) {
+                            const double chi = __dmul_rn(__dmul_rn(2.0, double(rest)),
+                                                         __dsub_rn(double(gmax), double(gmin)));
+                            const double num = __dmul_rn(__dmul_rn(8.0, __dmul_rn(chi, chi)), p.logmd);
+                            nrd = std_max(ceil(__ddiv_rn(num, dse2)), 1.0);
+                        }
+                        unsigned hb = __ballot_sync(kFullMask, has);
+                        while (hb) {  // rwcost += nr in slot order
+                            const int l = __ffs(hb) - 1;
+                            hb &= hb - 1;
+                            rw = __dadd_rn(rw, __shfl_sync(kFullMask, nrd, l));
+                        }
+                    }
+                });
+                lap(3);
+                if (picost >= __dmul_rn(25.0, rw)) break;
+                if (globaltimer_ns() > deadline) {
+                    timed_out = true;
+                    break;
                 }
-                const uint32_t cnt = min(32u, qs - i0);
-                uint32_t pt = 0, pc = 0;  // prefetch cursor: batch vertex, chunk offset
-                uint2 cur[kPushAhead];
-                uint32_t ct[kPushAhead], cco[kPushAhead];
-                auto load_group = [&](uint2* dst, uint32_t* dt, uint32_t* dc) {
-#pragma unroll
-                    for (int jj = 0; jj < kPushAhead; ++jj) {
-                        dst[jj] = make_uint2(0u, 1u);
-                        dt[jj] = cnt;
-                        dc[jj] = 0;
-                        if (pt < cnt) {
-                            const uint32_t vb = __shfl_sync(kFullMask, myb, pt);
-                            const uint32_t vd = __shfl_sync(kFullMask, myd, pt);
-                            if (pc + lane < vd) dst[jj] = __ldg(p.adjd + vb + pc + lane);
-                            dt[jj] = pt;
-                            dc[jj] = pc;
-                            pc += 32;
-                            if (pc >= vd) {
-                                ++pt;
-                                pc = 0;
-                            }
-                        }
-                    }
-                };
-                load_group(cur, ct, cco);
-                Real r = Real(0);
-                while (ct[0] < cnt) {
-                    uint2 nxt[kPushAhead];
-                    uint32_t nt[kPushAhead], nc[kPushAhead];
-                    load_group(nxt, nt, nc);
-#pragma unroll
-                    for (int jj = 0; jj < kPushAhead; ++jj) {
-                        if (ct[jj] < cnt) {
-                            const uint32_t t = ct[jj], c0 = cco[jj];
-                            const uint32_t vd = __shfl_sync(kFullMask, myd, t);
-                            if (c0 == 0) {
-                                const uint32_t v = __shfl_sync(kFullMask, myv, t);
-                                r = pvec[v];
-                                __syncwarp();
-                                if (lane == 0) pvec[v] = Real(0);
-                                __syncwarp();
-                                st_tr += vd;
-                            }
-                            const bool act = c0 + lane < vd;
-                            const uint32_t cu = cur[jj].x, cd = cur[jj].y;
-                            bool fresh = false;
-                            if (act && vis[cu] == 0) {
-                                vis[cu] = 1;
-                                fresh = true;
-                            }
-                            const unsigned bal = __ballot_sync(kFullMask, fresh);
-                            if (fresh) {
-                                qn[qns + __popc(bal & lt)] = cu;
-                                pcost += cd;
-                            }
-                            qns += __popc(bal);
-                            if (act) pvec[cu] = radd(pvec[cu], rdiv(r, from_u64<Real>(cd)));
-                            __syncwarp();
-                        }
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < kPushAhead; ++jj) {
-                        cur[jj] = nxt[jj];
-                        ct[jj] = nt[jj];
-                        cco[jj] = nc[jj];
-                    }
-                }
-            }
-            } else {
-                // ---- Jacobi push (mixed form) ----
-                // The frontier's residuals are taken together (r_i = pvec[q_i], pvec[q_i] = 0),
-                // then pushed over the concatenated adjacency of 32 frontier vertices at a time:
-                // each lane walks entries lane, lane + 32, ... with a cursor over the vertices'
-                // start offsets.  Two lanes of one step that reach the same neighbour apply their
-                // shares one after the other in lane order, so the result is deterministic.
+                uint32_t qns = 0;
+                pcost = 0;
+                st_pv += qs;
+                if constexpr (!JACOBI) {
+                // ---- diffuse (:218-239) ----
+                // The frontier is drained in order, one vertex at a time; the lanes share the
+                // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
+                // touch distinct bytes and words).  Per batch of 32 frontier vertices the adjacency is
+                // cut into 32-slot chunks walked by a cursor; a chunk's (neighbour, degree) pairs are
+                // one coalesced 8-byte load per lane, issued kPushAhead chunks before use.  picost (the
+                // new frontier's degree sum) is summed on discovery.  Every vertex has at least one
+                // chunk: tgtp_run rejects isolated vertices.
 
-                pipelined<uint32_t>(qs,
-                    [&](uint32_t i0, uint32_t* r) {
-#pragma unroll
-                        for (int b = 0; b < kB; ++b) {
-                            const uint32_t i = i0 + 32 * b + lane;
-                            r[b] = i < qs ? q[i] : NONE;
-                        }
-                    },
-                    [&](uint32_t i0, const uint32_t* r) {
-#pragma unroll
-                        for (int b = 0; b < kB; ++b) {
-                            if (r[b] == NONE) continue;
-                            p.rbuf[gw * size_t(n) + i0 + 32 * b + lane] = pvec[r[b]];
-                            pvec[r[b]] = Real(0);
-                        }
-                    });
-                __syncwarp();
-                uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64);
-                uint32_t* vbs = exs + 33;
-                Real* rvs = reinterpret_cast<Real*>(vbs + 32);
                 for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
-                    uint32_t vb = 0, vd = 0;
-                    Real rv = Real(0);
+                    uint32_t myv = 0, myb = 0, myd = 0;
                     if (i0 + lane < qs) {
-                        const uint32_t v = q[i0 + lane];
-                        vb = __ldg(idx + v);
-                        vd = __ldg(idx + v + 1) - vb;
-                        rv = p.rbuf[gw * size_t(n) + i0 + lane];
+                        myv = q[i0 + lane];
+                        myb = __ldg(idx + myv);
+                        myd = __ldg(idx + myv + 1) - myb;
                     }
-                    uint32_t incl = vd;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
-                        if (lane >= uint32_t(o)) incl += y;
-                    }
-                    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-                    exs[lane] = incl - vd;
-                    vbs[lane] = vb;
-                    rvs[lane] = rv;
-                    if (lane == 31) exs[32] = total;
-                    __syncwarp();
-                    st_tr += total;
-                    uint32_t cm = 0;
-                    struct PEnt {
-                        uint32_t seg, u, du;
-                    };
-                    pipelined<PEnt>(total,
-                        [&](uint32_t e0, PEnt* r) {
-#pragma unroll
-                            for (int b = 0; b < kB; ++b) {
-                                const uint32_t e = e0 + 32 * b + lane;
-                                r[b].seg = 32u;
-                                r[b].u = NONE;
-                                r[b].du = 1u;
-                                if (e < total) {
-                                    while (exs[cm + 1] <= e) ++cm;
-                                    const uint2 a = __ldg(p.adjd + vbs[cm] + (e - exs[cm]));
-                                    r[b].seg = cm;
-                                    r[b].u = a.x;
-                                    r[b].du = a.y;
+                    const uint32_t cnt = min(32u, qs - i0);
+                    uint32_t pt = 0, pc = 0;  // prefetch cursor: batch vertex, chunk offset
+                    uint2 cur[kPushAhead];
+                    uint32_t ct[kPushAhead], cco[kPushAhead];
+                    auto load_group = [&](uint2* dst, uint32_t* dt, uint32_t* dc) {
+    #pragma unroll
+                        for (int jj = 0; jj < kPushAhead; ++jj) {
+                            dst[jj] = make_uint2(0u, 1u);
+                            dt[jj] = cnt;
+                            dc[jj] = 0;
+                            if (pt < cnt) {
+                                const uint32_t vb = __shfl_sync(kFullMask, myb, pt);
+                                const uint32_t vd = __shfl_sync(kFullMask, myd, pt);
+                                if (pc + lane < vd) dst[jj] = __ldg(p.adjd + vb + pc + lane);
+                                dt[jj] = pt;
+                                dc[jj] = pc;
+                                pc += 32;
+                                if (pc >= vd) {
+                                    ++pt;
+                                    pc = 0;
                                 }
                             }
-                        },
-                        [&](uint32_t, const PEnt* r) {
-#pragma unroll
-                            for (int b = 0; b < kB; ++b) {
-                                const bool valid = r[b].seg < 32u;
-                                const uint32_t u = r[b].u;
-                                const Real share = valid ? rvs[r[b].seg] / from_u64<Real>(r[b].du) : Real(0);
-                                // entries of one frontier vertex are distinct neighbours; only a
-                                // step that spans several vertices can repeat one
-                                const uint32_t seg0 = __shfl_sync(kFullMask, r[b].seg, 0);
-                                const bool one_seg = __all_sync(kFullMask, !valid || r[b].seg == seg0);
-                                const unsigned grp =
-                                    one_seg ? (1u << lane) : __match_any_sync(kFullMask, u);
-                                const bool unique =
-                                    one_seg || __all_sync(kFullMask, !valid || grp == (1u << lane));
-                                if (unique) {
-                                    if (valid) pvec[u] = pvec[u] + share;
-                                } else {
-                                    for (uint32_t l = 0; l < 32; ++l) {
-                                        if (lane == l && valid) pvec[u] = pvec[u] + share;
-                                        __syncwarp();
-                                    }
+                        }
+                    };
+                    load_group(cur, ct, cco);
+                    Real r = Real(0);
+                    while (ct[0] < cnt) {
+                        uint2 nxt[kPushAhead];
+                        uint32_t nt[kPushAhead], nc[kPushAhead];
+                        load_group(nxt, nt, nc);
+    #pragma unroll
+                        for (int jj = 0; jj < kPushAhead; ++jj) {
+                            if (ct[jj] < cnt) {
+                                const uint32_t t = ct[jj], c0 = cco[jj];
+                                const uint32_t vd = __shfl_sync(kFullMask, myd, t);
+                                if (c0 == 0) {
+                                    const uint32_t v = __shfl_sync(kFullMask, myv, t);
+                                    r = pvec[v];
+                                    __syncwarp();
+                                    if (lane == 0) pvec[v] = Real(0);
+                                    __syncwarp();
+                                    st_tr += vd;
                                 }
-                                const bool leader = valid && lane == uint32_t(__ffs(grp) - 1);
+                                const bool act = c0 + lane < vd;
+                                const uint32_t cu = cur[jj].x, cd = cur[jj].y;
                                 bool fresh = false;
-                                if (leader && vis[u] == 0) {
-                                    vis[u] = 1;
+                                if (act && vis[cu] == 0) {
+                                    vis[cu] = 1;
                                     fresh = true;
                                 }
                                 const unsigned bal = __ballot_sync(kFullMask, fresh);
                                 if (fresh) {
-                                    qn[qns + __popc(bal & lt)] = u;
-                                    pcost += r[b].du;
+                                    qn[qns + __popc(bal & lt)] = cu;
+                                    pcost += cd;
                                 }
                                 qns += __popc(bal);
+                                if (act) pvec[cu] = radd(pvec[cu], rdiv(r, from_u64<Real>(cd)));
                                 __syncwarp();
+                            }
+                        }
+    #pragma unroll
+                        for (int jj = 0; jj < kPushAhead; ++jj) {
+                            cur[jj] = nxt[jj];
+                            ct[jj] = nt[jj];
+                            cco[jj] = nc[jj];
+                        }
+                    }
+                }
+                } else {
+                    // ---- Jacobi push (mixed form) ----
+                    // The frontier's residuals are taken together (r_i = pvec[q_i], pvec[q_i] = 0),
+                    // then pushed over the concatenated adjacency of 32 frontier vertices at a time:
+                    // each lane walks entries lane, lane + 32, ... with a cursor over the vertices'
+                    // start offsets.  Two lanes of one step that reach the same neighbour apply their
+                    // shares one after the other in lane order, so the result is deterministic.
+
+                    pipelined<uint32_t>(qs,
+                        [&](uint32_t i0, uint32_t* r) {
+    #pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const uint32_t i = i0 + 32 * b + lane;
+                                r[b] = i < qs ? q[i] : NONE;
+                            }
+                        },
+                        [&](uint32_t i0, const uint32_t* r) {
+    #pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                if (r[b] == NONE) continue;
+                                p.rbuf[gw * size_t(n) + i0 + 32 * b + lane] = pvec[r[b]];
+                                pvec[r[b]] = Real(0);
                             }
                         });
                     __syncwarp();
+                    uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64);
+                    uint32_t* vbs = exs + 33;
+                    Real* rvs = reinterpret_cast<Real*>(vbs + 32);
+                    for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
+                        uint32_t vb = 0, vd = 0;
+                        Real rv = Real(0);
+                        if (i0 + lane < qs) {
+                            const uint32_t v = q[i0 + lane];
+                            vb = __ldg(idx + v);
+                            vd = __ldg(idx + v + 1) - vb;
+                            rv = p.rbuf[gw * size_t(n) + i0 + lane];
+                        }
+                        uint32_t incl = vd;
+    #pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                            if (lane >= uint32_t(o)) incl += y;
+                        }
+                        const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                        exs[lane] = incl - vd;
+                        vbs[lane] = vb;
+                        rvs[lane] = rv;
+                        if (lane == 31) exs[32] = total;
+                        __syncwarp();
+                        st_tr += total;
+                        uint32_t cm = 0;
+                        struct PEnt {
+                            uint32_t seg, u, du;
+                        };
+                        pipelined<PEnt>(total,
+                            [&](uint32_t e0, PEnt* r) {
+    #pragma unroll
+                                for (int b = 0; b < kB; ++b) {
+                                    const uint32_t e = e0 + 32 * b + lane;
+                                    r[b].seg = 32u;
+                                    r[b].u = NONE;
+                                    r[b].du = 1u;
+                                    if (e < total) {
+                                        while (exs[cm + 1] <= e) ++cm;
+                                        const uint2 a = __ldg(p.adjd + vbs[cm] + (e - exs[cm]));
+                                        r[b].seg = cm;
+                                        r[b].u = a.x;
+                                        r[b].du = a.y;
+                                    }
+                                }
+                            },
+                            [&](uint32_t, const PEnt* r) {
+    #pragma unroll
+                                for (int b = 0; b < kB; ++b) {
+                                    const bool valid = r[b].seg < 32u;
+                                    const uint32_t u = r[b].u;
+                                    const Real share = valid ? rvs[r[b].seg] / from_u64<Real>(r[b].du) : Real(0);
+                                    // entries of one frontier vertex are distinct neighbours; only a
+                                    // step that spans several vertices can repeat one
+                                    const uint32_t seg0 = __shfl_sync(kFullMask, r[b].seg, 0);
+                                    const bool one_seg = __all_sync(kFullMask, !valid || r[b].seg == seg0);
+                                    const unsigned grp =
+                                        one_seg ? (1u << lane) : __match_any_sync(kFullMask, u);
+                                    const bool unique =
+                                        one_seg || __all_sync(kFullMask, !valid || grp == (1u << lane));
+                                    if (unique) {
+                                        if (valid) pvec[u] = pvec[u] + share;
+                                    } else {
+                                        for (uint32_t l = 0; l < 32; ++l) {
+                                            if (lane == l && valid) pvec[u] = pvec[u] + share;
+                                            __syncwarp();
+                                        }
+                                    }
+                                    const bool leader = valid && lane == uint32_t(__ffs(grp) - 1);
+                                    bool fresh = false;
+                                    if (leader && vis[u] == 0) {
+                                        vis[u] = 1;
+                                        fresh = true;
+                                    }
+                                    const unsigned bal = __ballot_sync(kFullMask, fresh);
+                                    if (fresh) {
+                                        qn[qns + __popc(bal & lt)] = u;
+                                        pcost += r[b].du;
+                                    }
+                                    qns += __popc(bal);
+                                    __syncwarp();
+                                }
+                            });
+                        __syncwarp();
+                    }
                 }
-            }
-            __syncwarp();
-            lap(1);
-            // preds[row] += (pvec[src] - pvec[adj]) / ds (:235-237); the first round adds to the
-            // initial 1 / ds directly
-            {
-                const Real ps = pvec[src];
-                struct SlotPred {
-                    uint32_t w;
-                    Acc old;
-                };
-                pipelined<SlotPred>(dsi,
-                    [&](uint32_t c, SlotPred* r) {
-#pragma unroll
-                        for (int b = 0; b < kB; ++b) {
-                            const uint32_t o = c + 32 * b + lane;
-                            r[b].w = NONE;
-                            r[b].old = pinit;
-                            if (o < dsi) {
-                                r[b].w = __ldg(adj + rb + o);
-                                if (ell > 0) r[b].old = p.preds[rb + o];
+                __syncwarp();
+                lap(1);
+                // preds[row] += (pvec[src] - pvec[adj]) / ds (:235-237); the first round adds to the
+                // initial 1 / ds directly
+                {
+                    const Real ps = pvec[src];
+                    struct SlotPred {
+                        uint32_t w;
+                        Acc old;
+                    };
+                    pipelined<SlotPred>(dsi,
+                        [&](uint32_t c, SlotPred* r) {
+    #pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const uint32_t o = c + 32 * b + lane;
+                                r[b].w = NONE;
+                                r[b].old = pinit;
+                                if (o < dsi) {
+                                    r[b].w = __ldg(adj + rb + o);
+                                    if (ell > 0) r[b].old = p.preds[rb + o];
+                                }
                             }
+                        },
+                        [&](uint32_t c, const SlotPred* r) {
+    #pragma unroll
+                            for (int b = 0; b < kB; ++b)
+                                if (r[b].w != NONE)
+                                    p.preds[rb + c + 32 * b + lane] =
+                                        row_update<Real, Acc>(r[b].old, ps, pvec[r[b].w], ds);
+                        });
+                }
+                // clear the new frontier's flags and take its residual max / min (:484-491; max and
+                // min do not depend on order)
+                mx = Real(0);
+                mn = Real(1);
+                pipelined<uint32_t>(qns,
+                    [&](uint32_t i0, uint32_t* r) {
+    #pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            r[b] = i < qns ? qn[i] : NONE;
                         }
                     },
-                    [&](uint32_t c, const SlotPred* r) {
-#pragma unroll
-                        for (int b = 0; b < kB; ++b)
-                            if (r[b].w != NONE)
-                                p.preds[rb + c + 32 * b + lane] =
-                                    row_update<Real, Acc>(r[b].old, ps, pvec[r[b].w], ds);
+                    [&](uint32_t, const uint32_t* r) {
+    #pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            if (r[b] == NONE) continue;
+                            vis[r[b]] = 0;
+                            const Real val = pvec[r[b]];
+                            mx = std_max(mx, val);
+                            mn = std_min(mn, val);
+                        }
                     });
+                __syncwarp();
+                { uint32_t* tmp = q; q = qn; qn = tmp; }
+                qs = qns;
+                ++ell;
+                lap(2);
             }
-            // clear the new frontier's flags and take its residual max / min (:484-491; max and
-            // min do not depend on order)
-            mx = Real(0);
-            mn = Real(1);
-            pipelined<uint32_t>(qns,
-                [&](uint32_t i0, uint32_t* r) {
-#pragma unroll
-                    for (int b = 0; b < kB; ++b) {
-                        const uint32_t i = i0 + 32 * b + lane;
-                        r[b] = i < qns ? qn[i] : NONE;
-                    }
-                },
-                [&](uint32_t, const uint32_t* r) {
-#pragma unroll
-                    for (int b = 0; b < kB; ++b) {
-                        if (r[b] == NONE) continue;
-                        vis[r[b]] = 0;
-                        const Real val = pvec[r[b]];
-                        mx = std_max(mx, val);
-                        mn = std_min(mn, val);
-                    }
-                });
-            __syncwarp();
-            { uint32_t* tmp = q; q = qn; qn = tmp; }
-            qs = qns;
-            ++ell;
-            lap(2);
         }
         if (timed_out) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);
             break;
         }
-        st_rounds += ell;
+        if (!p.pre) st_rounds += ell;  // PrePush rounds are counted by push_block_kernel
 
         // slots that still need walks (rest = tau - ell > 0), compacted in slot order
         uint32_t nitems = 0;
@@ -1863,7 +2163,22 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     grow(g, g->preds, sizeof(Acc) * (m + 1));
     // one zeroing for the striped counters, the work words and the row marks behind them
     const size_t stat_bytes = sizeof(unsigned long long) * kStCount * kStStripes;
-    const size_t zero_bytes = stat_bytes + sizeof(unsigned) * (4 + n + 1);
+    // mixed form, residual vectors too large for shared memory: multi-source push in waves of
+    // block_ctas x kBlockCols listed sources (each wave has its own claim counter)
+    const size_t per_warp_smem = ((size_t(n) * sizeof(Real) + 15) & ~size_t(15)) +
+                                 ((size_t(n) + 15) & ~size_t(15)) + kAccBytes;
+    bool block_mode = JACOBI && per_warp_smem > size_t(112) * 1024;
+    if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
+    uint32_t block_ctas = uint32_t(g->num_sms);
+    {
+        const size_t per_cta = 2 * size_t(n) * kBlockCols * sizeof(float);
+        const size_t budget = size_t(24) << 30;
+        block_ctas = uint32_t(std::max<size_t>(1, std::min<size_t>(block_ctas, budget / per_cta)));
+    }
+    const uint32_t waves =
+        block_mode ? uint32_t((n + uint64_t(block_ctas) * kBlockCols - 1) / (uint64_t(block_ctas) * kBlockCols))
+                   : 0u;
+    const size_t zero_bytes = stat_bytes + sizeof(unsigned) * (4 + n + 1 + waves);
     grow(g, g->stats, zero_bytes);
     auto* stats = g->stats.as<unsigned long long>();
     auto* work = run_work(g);
@@ -1996,10 +2311,75 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.stats = stats;
     p.adjd = g->adjd.as<uint2>();
     p.budget_ns = deadline_from_env();
-    {
+    p.pre = nullptr;
+    p.pre_cols = nullptr;
+    p.pre_final = nullptr;
+    if (!block_mode) {
+        p.claim = work;
+        p.list_base = 0;
+        p.list_cap = uint32_t(n);
         ScopedKernel k(g->prof, s, "source");
         launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
         TGTP_LAUNCH_CHECK("source_kernel");
+    } else {
+        grow(g, g->block_cols, 2 * size_t(n) * kBlockCols * sizeof(float) * block_ctas);
+        grow(g, g->block_pre, sizeof(PrePush) * (n + 1));
+        grow(g, g->block_final, sizeof(uint32_t) * (block_ctas + 1));
+        PushBlockParams bp;
+        bp.idx = p.idx;
+        bp.adj = p.adj;
+        bp.deg = p.deg;
+        bp.adjd = p.adjd;
+        bp.n = uint32_t(n);
+        bp.taus = p.taus;
+        bp.preds = reinterpret_cast<double*>(p.preds);
+        bp.work = work;
+        bp.rows = rm.list;
+        bp.eps = cfg.epsilon;
+        bp.logmd = logmd;
+        bp.cols = g->block_cols.as<float>();
+        bp.final_buf = g->block_final.as<uint32_t>();
+        bp.pre = g->block_pre.as<PrePush>();
+        bp.stats = stats;
+        bp.budget_ns = p.budget_ns;
+        p.pre = bp.pre;
+        p.pre_cols = bp.cols;
+        p.pre_final = bp.final_buf;
+        // the listed rows ordered by their largest tau (unlisted rows sort last, key 0)
+        grow(g, g->block_keys, sizeof(uint32_t) * 4 * (n + 1));
+        uint32_t* key = g->block_keys.as<uint32_t>();
+        uint32_t* ids = key + (n + 1);
+        uint32_t* skey = ids + (n + 1);
+        uint32_t* sorted = skey + (n + 1);
+        size_t tbytes = 0;
+        TGTP_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tbytes, key, skey, ids, sorted,
+                                                            int(n), 0, 32, s));
+        grow(g, g->block_tmp, tbytes + 16);
+        {
+            ScopedKernel k(g->prof, s, "row_key");
+            launch(row_key_kernel, grid_cap(uint64_t(n) * 32, 256, g->num_sms, 8), 256u, size_t(0), s,
+                   true, g->idx.as<uint32_t>(), g->taus.as<int>(), rm.mark, uint32_t(n), key, ids);
+            TGTP_LAUNCH_CHECK("row_key_kernel");
+        }
+        TGTP_CUDA(cub::DeviceRadixSort::SortPairsDescending(g->block_tmp.ptr, tbytes, key, skey, ids,
+                                                            sorted, int(n), 0, 32, s));
+        bp.rows = sorted;
+        p.rows = sorted;
+        unsigned* claims = work + 4 + n + 1;
+        for (uint32_t w = 0; w < waves; ++w) {
+            bp.base = w * block_ctas * kBlockCols;
+            {
+                ScopedKernel k(g->prof, s, "push_block");
+                launch(push_block_kernel, block_ctas, 1024u, size_t(0), s, true, bp);
+                TGTP_LAUNCH_CHECK("push_block_kernel");
+            }
+            p.claim = claims + w;
+            p.list_base = bp.base;
+            p.list_cap = block_ctas * kBlockCols;
+            ScopedKernel k(g->prof, s, "source");
+            launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
+            TGTP_LAUNCH_CHECK("source_kernel");
+        }
     }
     {
         ScopedKernel k(g->prof, s, "finish");
