@@ -85,3 +85,29 @@ def test_mixed_matches_fp64_when_no_walks_run(cuda_device, config1_inputs):
         assert a.stats()["walk_edges"] == 0
         np.testing.assert_allclose(mixed, f64, rtol=1e-5, atol=0)
     g.free()
+
+
+@pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
+def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, monkeypatch):
+    """The per-warp push and the multi-source block push sum residuals in fixed point, so the two
+    give identical scores, taus and work counters."""
+    from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_MIXED, VEC_BF16, VEC_F32
+
+    c = golden_tgtp_case(manifest, name)
+    g = _graph(c)
+    for run in c["runs"]:
+        for vd in (VEC_F32, VEC_BF16):
+            got = {}
+            for block in ("0", "1"):
+                monkeypatch.setenv("TGTP_MIXED_BLOCK", block)
+                a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"],
+                                       precision=PRECISION_MIXED, vec_dtype=vd))
+                s = a.tgtp()
+                st = a.stats()
+                got[block] = (s, a.taus(), {k: st[k] for k in ("push_rounds", "push_vertices",
+                                                               "push_traversals", "walk_edges",
+                                                               "walk_count", "walk_hops")})
+            assert np.array_equal(got["0"][0].view(np.uint32), got["1"][0].view(np.uint32)), run
+            assert np.array_equal(got["0"][1], got["1"][1])
+            assert got["0"][2] == got["1"][2], (run, got["0"][2], got["1"][2])
+    g.free()

@@ -64,6 +64,7 @@ constexpr int kStStripes = 32;
 // MIXED over BF16 rows.  A layout is (kLayoutSmem if the residual vectors live in shared memory) |
 // warps per block; 0 = the default rule.
 constexpr uint16_t kLayoutSmem = 0x100;
+constexpr uint16_t kLayoutBlock = 0x200;  // mixed form: multi-source block push
 inline int form_key(const tgtp_config& cfg) {
     if (cfg.precision == TGTP_PRECISION_FP32) return 0;
     if (cfg.precision == TGTP_PRECISION_FP64) return 1;
@@ -344,6 +345,19 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
     const float bp = __fsub_rn(s, a);
     e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+
+// Residual arithmetic of the mixed form's push: the residual a vertex u receives in a round is the
+// exact integer sum of its frontier neighbours' residuals in 2^-62 fixed point, divided (rounding
+// down) by deg(u), then rounded once to FP32.  The sum does not depend on the order of the
+// additions, so the per-warp push and the multi-source block push give the same bits.  Residuals
+// never exceed 1 and a round conserves their total, so no sum exceeds 2^62.
+constexpr unsigned long long kFixOne = 1ull << 62;
+__device__ __forceinline__ unsigned long long to_fixed(float r) {
+    return __float2ull_rn(__fmul_rn(r, 0x1p62f));
+}
+__device__ __forceinline__ float from_fixed(unsigned long long s, uint32_t d) {
+    return __fmul_rn(__ull2float_rn(s / d), 0x1p-62f);
 }
 
 __device__ __forceinline__ float vec_load(const float* p) { return __ldg(p); }
@@ -710,7 +724,8 @@ struct SourceParams {
     uint32_t* qbuf;       // 2 * n per warp
     WalkItem* items;      // max_degree per warp
     Real* pvec_g;         // n per warp (global tier)
-    Real* rbuf;           // n per warp: frontier residuals taken together (Jacobi push)
+    unsigned long long* rbuf;  // n per warp: frontier residuals in fixed point (Jacobi push)
+    unsigned long long* fx_g;  // n per warp: fixed-point accumulators (Jacobi push, global tier)
     unsigned char* vis_g; // vis_stride per warp (global tier)
     size_t vis_stride;
     size_t smem_per_warp;
@@ -969,7 +984,7 @@ push_block_kernel(PushBlockParams p) {
         float mx = 0.f, mn = 1.f;
         for (uint32_t o = lane; o < dsi; o += 32) {
             const uint2 a = __ldg(p.adjd + rb + o);
-            const float pu = __fdiv_rn(1.f, float(a.y));
+            const float pu = from_fixed(kFixOne, a.y);
             A[size_t(a.x) * S + j] = pu;
             pc += a.y;
             mx = fmaxf(mx, pu);
@@ -1060,7 +1075,7 @@ push_block_kernel(PushBlockParams p) {
         float mx = 0.f, mn = 1.f;
         for (uint32_t u = warp; u < n; u += nwarp) {
             const uint32_t ub = __ldg(p.idx + u), ud = __ldg(p.idx + u + 1) - ub;
-            float acc = 0.f;
+            unsigned long long acc = 0;
             for (uint32_t c = 0; c < ud; c += 32) {
                 const uint32_t nb = c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u;
                 const uint32_t k = min(32u, ud - c);
@@ -1070,13 +1085,13 @@ push_block_kernel(PushBlockParams p) {
                     const float x1 = cur[size_t(__shfl_sync(kFullMask, nb, t + 1)) * S + lane];
                     const float x2 = cur[size_t(__shfl_sync(kFullMask, nb, t + 2)) * S + lane];
                     const float x3 = cur[size_t(__shfl_sync(kFullMask, nb, t + 3)) * S + lane];
-                    acc = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(acc, x0), x1), x2), x3);
+                    acc += to_fixed(x0) + to_fixed(x1) + to_fixed(x2) + to_fixed(x3);
                 }
-                for (; t < k; ++t) acc = __fadd_rn(acc, cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane]);
+                for (; t < k; ++t) acc += to_fixed(cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane]);
             }
             float r = cur[size_t(u) * S + lane];
             if (run) {
-                r = acc > 0.f ? __fdiv_rn(acc, float(ud)) : 0.f;
+                r = acc ? from_fixed(acc, ud) : 0.f;
                 if (r > 0.f) {
                     pc += ud;
                     ++sup;
@@ -1160,15 +1175,20 @@ source_kernel(SourceParams<Real, Acc> p) {
     Real* pvec;
     unsigned char* vis;       // per vertex: 1 = discovered this round, 2 = in the top-gamma set
     unsigned long long* acc;  // 64 per warp: per-slot neighbourhood max (0..31) / min (32..63)
+    unsigned long long* fx;   // Jacobi push: per-vertex fixed-point accumulators (all zero between rounds)
     if (SMEM) {
         unsigned char* base = smem + size_t(wib) * p.smem_per_warp;
         pvec = reinterpret_cast<Real*>(base);
         const size_t pv = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
         vis = base + pv;
-        acc = reinterpret_cast<unsigned long long*>(base + pv + ((size_t(n) + 15) & ~size_t(15)));
+        const size_t vb = (size_t(n) + 15) & ~size_t(15);
+        fx = reinterpret_cast<unsigned long long*>(base + pv + vb);
+        acc = reinterpret_cast<unsigned long long*>(base + pv + vb +
+                                                    (JACOBI ? sizeof(unsigned long long) * n : 0));
     } else {
         pvec = p.pvec_g + gw * size_t(n);
         vis = p.vis_g + gw * p.vis_stride;
+        fx = JACOBI ? p.fx_g + gw * size_t(n) : nullptr;
         acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
     bool cleared = false;  // pvec and flags are zeroed once, before the warp's first source
@@ -1219,6 +1239,7 @@ source_kernel(SourceParams<Real, Acc> p) {
             for (uint32_t i = lane; i < n; i += 32) {
                 pvec[i] = Real(0);
                 vis[i] = 0;
+                if (JACOBI) fx[i] = 0ull;
             }
             cleared = true;
             __syncwarp();
@@ -1296,7 +1317,8 @@ source_kernel(SourceParams<Real, Acc> p) {
                     for (int b = 0; b < kB; ++b) {
                         if (r[b].x == NONE) continue;
                         const uint32_t o = c + 32 * b + lane;
-                        const Real pu = rdiv(Real(1), from_u64<Real>(r[b].y));
+                        const Real pu = JACOBI ? Real(from_fixed(kFixOne, r[b].y))
+                                               : rdiv(Real(1), from_u64<Real>(r[b].y));
                         pvec[r[b].x] = pu;
                         qn[o] = r[b].x;
                         pcost += r[b].y;
@@ -1438,43 +1460,46 @@ source_kernel(SourceParams<Real, Acc> p) {
                 }
                 } else {
                     // ---- Jacobi push (mixed form) ----
-                    // The frontier's residuals are taken together (r_i = pvec[q_i], pvec[q_i] = 0),
-                    // then pushed over the concatenated adjacency of 32 frontier vertices at a time:
-                    // each lane walks entries lane, lane + 32, ... with a cursor over the vertices'
-                    // start offsets.  Two lanes of one step that reach the same neighbour apply their
-                    // shares one after the other in lane order, so the result is deterministic.
-
+                    // The frontier's residuals are taken together, in 2^-62 fixed point
+                    // (r_i = to_fixed(pvec[q_i]), pvec[q_i] = 0), then pushed over the concatenated
+                    // adjacency of 32 frontier vertices at a time: each lane walks entries lane,
+                    // lane + 32, ... with a cursor over the vertices' start offsets, and every entry
+                    // (v -> u) adds r_v to u's 64-bit accumulator with an integer atomic, so the sums
+                    // do not depend on the order.  The touched vertices form the new frontier in
+                    // discovery order; once the round is over their residuals become
+                    // acc[u] / deg(u) (from_fixed), exactly as push_block_kernel computes them.
+                    unsigned long long* rfx = p.rbuf + gw * size_t(n);
                     pipelined<uint32_t>(qs,
                         [&](uint32_t i0, uint32_t* r) {
-    #pragma unroll
+#pragma unroll
                             for (int b = 0; b < kB; ++b) {
                                 const uint32_t i = i0 + 32 * b + lane;
                                 r[b] = i < qs ? q[i] : NONE;
                             }
                         },
                         [&](uint32_t i0, const uint32_t* r) {
-    #pragma unroll
+#pragma unroll
                             for (int b = 0; b < kB; ++b) {
                                 if (r[b] == NONE) continue;
-                                p.rbuf[gw * size_t(n) + i0 + 32 * b + lane] = pvec[r[b]];
+                                rfx[i0 + 32 * b + lane] = to_fixed(float(pvec[r[b]]));
                                 pvec[r[b]] = Real(0);
                             }
                         });
                     __syncwarp();
-                    uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64);
+                    unsigned long long* rvs = acc + 64;
+                    uint32_t* exs = reinterpret_cast<uint32_t*>(rvs + 32);
                     uint32_t* vbs = exs + 33;
-                    Real* rvs = reinterpret_cast<Real*>(vbs + 32);
                     for (uint32_t i0 = 0; i0 < qs; i0 += 32) {
                         uint32_t vb = 0, vd = 0;
-                        Real rv = Real(0);
+                        unsigned long long rv = 0;
                         if (i0 + lane < qs) {
                             const uint32_t v = q[i0 + lane];
                             vb = __ldg(idx + v);
                             vd = __ldg(idx + v + 1) - vb;
-                            rv = p.rbuf[gw * size_t(n) + i0 + lane];
+                            rv = rfx[i0 + lane];
                         }
                         uint32_t incl = vd;
-    #pragma unroll
+#pragma unroll
                         for (int o = 1; o < 32; o <<= 1) {
                             const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
                             if (lane >= uint32_t(o)) incl += y;
@@ -1492,7 +1517,7 @@ source_kernel(SourceParams<Real, Acc> p) {
                         };
                         pipelined<PEnt>(total,
                             [&](uint32_t e0, PEnt* r) {
-    #pragma unroll
+#pragma unroll
                                 for (int b = 0; b < kB; ++b) {
                                     const uint32_t e = e0 + 32 * b + lane;
                                     r[b].seg = 32u;
@@ -1508,27 +1533,18 @@ source_kernel(SourceParams<Real, Acc> p) {
                                 }
                             },
                             [&](uint32_t, const PEnt* r) {
-    #pragma unroll
+#pragma unroll
                                 for (int b = 0; b < kB; ++b) {
                                     const bool valid = r[b].seg < 32u;
                                     const uint32_t u = r[b].u;
-                                    const Real share = valid ? rvs[r[b].seg] / from_u64<Real>(r[b].du) : Real(0);
+                                    if (valid) atomicAdd(fx + u, rvs[r[b].seg]);
                                     // entries of one frontier vertex are distinct neighbours; only a
-                                    // step that spans several vertices can repeat one
+                                    // step that spans several vertices can repeat one, and then the
+                                    // first lane of a repeated neighbour discovers it
                                     const uint32_t seg0 = __shfl_sync(kFullMask, r[b].seg, 0);
                                     const bool one_seg = __all_sync(kFullMask, !valid || r[b].seg == seg0);
                                     const unsigned grp =
                                         one_seg ? (1u << lane) : __match_any_sync(kFullMask, u);
-                                    const bool unique =
-                                        one_seg || __all_sync(kFullMask, !valid || grp == (1u << lane));
-                                    if (unique) {
-                                        if (valid) pvec[u] = pvec[u] + share;
-                                    } else {
-                                        for (uint32_t l = 0; l < 32; ++l) {
-                                            if (lane == l && valid) pvec[u] = pvec[u] + share;
-                                            __syncwarp();
-                                        }
-                                    }
                                     const bool leader = valid && lane == uint32_t(__ffs(grp) - 1);
                                     bool fresh = false;
                                     if (leader && vis[u] == 0) {
@@ -1546,6 +1562,23 @@ source_kernel(SourceParams<Real, Acc> p) {
                             });
                         __syncwarp();
                     }
+                    // the touched vertices' new residuals
+                    pipelined<uint32_t>(qns,
+                        [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const uint32_t i = i0 + 32 * b + lane;
+                                r[b] = i < qns ? qn[i] : NONE;
+                            }
+                        },
+                        [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                if (r[b] == NONE) continue;
+                                pvec[r[b]] = Real(from_fixed(fx[r[b]], __ldg(p.deg + r[b])));
+                                fx[r[b]] = 0ull;
+                            }
+                        });
                 }
                 __syncwarp();
                 lap(1);
@@ -1980,7 +2013,10 @@ template <class Real, class Acc>
 __device__ __forceinline__ Acc closed_row_score(uint32_t ds, uint32_t du) {
     const Real d = from_u64<Real>(ds);
     const Acc pinit = from_f64<Acc>(__ddiv_rn(1.0, double(d)));
-    return row_update<Real, Acc>(pinit, Real(0), rdiv(Real(1), from_u64<Real>(du)), d);
+    // the mixed form (FP32 residuals, FP64 scores) forms 1 / deg(u) as its push does
+    constexpr bool kMixed = std::is_same<Real, float>::value && std::is_same<Acc, double>::value;
+    const Real pu = kMixed ? Real(from_fixed(kFixOne, du)) : rdiv(Real(1), from_u64<Real>(du));
+    return row_update<Real, Acc>(pinit, Real(0), pu, d);
 }
 
 template <class Real, class Acc>
@@ -2165,10 +2201,13 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     const size_t stat_bytes = sizeof(unsigned long long) * kStCount * kStStripes;
     // mixed form, residual vectors too large for shared memory: multi-source push in waves of
     // block_ctas x kBlockCols listed sources (each wave has its own claim counter)
-    const size_t per_warp_smem = ((size_t(n) * sizeof(Real) + 15) & ~size_t(15)) +
-                                 ((size_t(n) + 15) & ~size_t(15)) + kAccBytes;
-    bool block_mode = JACOBI && per_warp_smem > size_t(112) * 1024;
-    if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
+    // The block push gives the same bits as the per-warp push (fixed-point residual sums), so the
+    // choice is only about speed: the handle's tuned layout, else TGTP_MIXED_BLOCK, else the
+    // per-warp push.
+    const int key = form_key(cfg);
+    bool block_mode = false;
+    if (g->src_layout[key]) block_mode = JACOBI && (g->src_layout[key] & kLayoutBlock) != 0;
+    else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
     uint32_t block_ctas = uint32_t(g->num_sms);
     {
         const size_t per_cta = 2 * size_t(n) * kBlockCols * sizeof(float);
@@ -2249,13 +2288,13 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     // TGTP_PVEC_TIER=smem|global overrides the tier of the default rule.
     const size_t pv_bytes = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
     const size_t vis_bytes = (size_t(n) + 15) & ~size_t(15);
-    const size_t per_warp = pv_bytes + vis_bytes + kAccBytes;
-    const int key = form_key(cfg);
+    const size_t fx_bytes = JACOBI ? sizeof(unsigned long long) * size_t(n) : 0;
+    const size_t per_warp = pv_bytes + vis_bytes + fx_bytes + kAccBytes;
     bool use_smem;
     int wpb;
     if (g->src_layout[key]) {
         use_smem = (g->src_layout[key] & kLayoutSmem) != 0;
-        wpb = g->src_layout[key] & 0xff;
+        wpb = std::max(1, g->src_layout[key] & 0xff);
     } else {
         use_smem = per_warp <= size_t(112) * 1024;
         if (const char* t = std::getenv("TGTP_PVEC_TIER")) {
@@ -2279,10 +2318,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t q_bytes = align(warps * 2 * size_t(n) * 4);
     const size_t it_bytes = align(warps * maxd * sizeof(WalkItem));
-    const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(Real)) : 0;
+    const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(unsigned long long)) : 0;
     const size_t pvg_bytes = use_smem ? 0 : align(warps * size_t(n) * sizeof(Real));
     const size_t visg_bytes = use_smem ? 0 : align(warps * vis_bytes);
-    grow(g, g->scratch, q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + 256);
+    const size_t fxg_bytes = (JACOBI && !use_smem) ? align(warps * fx_bytes) : 0;
+    grow(g, g->scratch, q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
     SourceParams<Real, Acc> p;
     p.idx = g->idx.as<uint32_t>();
@@ -2297,11 +2337,13 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     base += q_bytes;
     p.items = reinterpret_cast<WalkItem*>(base);
     base += it_bytes;
-    p.rbuf = JACOBI ? reinterpret_cast<Real*>(base) : nullptr;
+    p.rbuf = JACOBI ? reinterpret_cast<unsigned long long*>(base) : nullptr;
     base += rb_bytes;
     p.pvec_g = use_smem ? nullptr : reinterpret_cast<Real*>(base);
     base += pvg_bytes;
     p.vis_g = use_smem ? nullptr : base;
+    base += visg_bytes;
+    p.fx_g = fxg_bytes ? reinterpret_cast<unsigned long long*>(base) : nullptr;
     p.vis_stride = vis_bytes;
     p.smem_per_warp = per_warp;
     p.max_degree = uint32_t(maxd);
@@ -2447,11 +2489,17 @@ void aesc_check_flags(tgtp_graph* g) {
 int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials) {
     const int key = form_key(cfg);
     const size_t rs = cfg.precision == TGTP_PRECISION_FP64 ? 8 : 4;
-    const size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
+    const bool mixed = cfg.precision == TGTP_PRECISION_MIXED;
+    const size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) +
+                            (mixed ? 8 * g->n : 0) + kAccBytes;
     std::vector<uint16_t> cand;
     for (int w : {1, 2})
         if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(kLayoutSmem | w));
     for (int w : {1, 2, 4}) cand.push_back(uint16_t(w));
+    if (mixed) {  // the block push, with the per-source stage in the best layout that fits
+        const uint16_t post = per_warp <= size_t(112) * 1024 ? uint16_t(kLayoutSmem | 1) : uint16_t(4);
+        cand.push_back(uint16_t(kLayoutBlock | post));
+    }
     cudaEvent_t e0, e1;
     TGTP_CUDA(cudaEventCreate(&e0));
     TGTP_CUDA(cudaEventCreate(&e1));
