@@ -1182,9 +1182,13 @@ source_kernel(SourceParams<Real, Acc> p) {
         const size_t pv = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
         vis = base + pv;
         const size_t vb = (size_t(n) + 15) & ~size_t(15);
-        fx = reinterpret_cast<unsigned long long*>(base + pv + vb);
+        // the fixed-point accumulators live in shared memory when they fit beside the residual
+        // vector, else in HBM (p.fx_g)
+        const bool fx_here = JACOBI && p.fx_g == nullptr;
+        fx = fx_here ? reinterpret_cast<unsigned long long*>(base + pv + vb)
+                     : (JACOBI ? p.fx_g + gw * size_t(n) : nullptr);
         acc = reinterpret_cast<unsigned long long*>(base + pv + vb +
-                                                    (JACOBI ? sizeof(unsigned long long) * n : 0));
+                                                    (fx_here ? sizeof(unsigned long long) * n : 0));
     } else {
         pvec = p.pvec_g + gw * size_t(n);
         vis = p.vis_g + gw * p.vis_stride;
@@ -2202,12 +2206,14 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     // mixed form, residual vectors too large for shared memory: multi-source push in waves of
     // block_ctas x kBlockCols listed sources (each wave has its own claim counter)
     // The block push gives the same bits as the per-warp push (fixed-point residual sums), so the
-    // choice is only about speed: the handle's tuned layout, else TGTP_MIXED_BLOCK, else the
-    // per-warp push.
+    // choice is only about speed: the handle's tuned layout, else TGTP_MIXED_BLOCK, else what the
+    // last completed mixed run on this graph measured (push_hint), else the per-warp push.
     const int key = form_key(cfg);
     bool block_mode = false;
     if (g->src_layout[key]) block_mode = JACOBI && (g->src_layout[key] & kLayoutBlock) != 0;
     else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
+    else block_mode = JACOBI && g->push_hint[key] == 2;
+    g->last_key = key;
     uint32_t block_ctas = uint32_t(g->num_sms);
     {
         const size_t per_cta = 2 * size_t(n) * kBlockCols * sizeof(float);
@@ -2289,7 +2295,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     const size_t pv_bytes = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
     const size_t vis_bytes = (size_t(n) + 15) & ~size_t(15);
     const size_t fx_bytes = JACOBI ? sizeof(unsigned long long) * size_t(n) : 0;
-    const size_t per_warp = pv_bytes + vis_bytes + fx_bytes + kAccBytes;
+    // the mixed form's fixed-point accumulators join the shared-memory copy only while the three
+    // arrays fit in 112 KB; beyond that they move to HBM and the residual vector stays in shared
+    // memory up to the same size as in the other forms
+    const bool fx_in_smem = JACOBI && pv_bytes + vis_bytes + fx_bytes + kAccBytes <= size_t(112) * 1024;
+    const size_t per_warp = pv_bytes + vis_bytes + (fx_in_smem ? fx_bytes : 0) + kAccBytes;
     bool use_smem;
     int wpb;
     if (g->src_layout[key]) {
@@ -2321,7 +2331,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(unsigned long long)) : 0;
     const size_t pvg_bytes = use_smem ? 0 : align(warps * size_t(n) * sizeof(Real));
     const size_t visg_bytes = use_smem ? 0 : align(warps * vis_bytes);
-    const size_t fxg_bytes = (JACOBI && !use_smem) ? align(warps * fx_bytes) : 0;
+    const size_t fxg_bytes = (JACOBI && !(use_smem && fx_in_smem)) ? align(warps * fx_bytes) : 0;
     grow(g, g->scratch, q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
     SourceParams<Real, Acc> p;
@@ -2486,12 +2496,33 @@ void aesc_check_flags(tgtp_graph* g) {
         fail(TGTP_ERR_UNSUPPORTED, "a walk count exceeds the 32-bit walk grid");
 }
 
+void aesc_read_stats(tgtp_graph* g, unsigned long long* st) {
+    unsigned long long stripes[kStCount * kStStripes];
+    TGTP_CUDA(cudaMemcpyAsync(stripes, g->stats.ptr, sizeof(stripes), cudaMemcpyDeviceToHost,
+                              g->stream));
+    TGTP_CUDA(cudaStreamSynchronize(g->stream));
+    for (int i = 0; i < kStCount; ++i) st[i] = 0;
+    for (int c = 0; c < kStStripes; ++c)
+        for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
+    // Mixed form: a dense round of the block push reads every slot once per 32 sources, about 40
+    // times cheaper per slot than a per-warp push reads a frontier entry (scattered residual
+    // updates in HBM).  So the block push pays off when a round's frontier averages more than
+    // m / 40 traversals -- for graphs whose residual vectors do not fit in shared memory (smaller
+    // ones push per warp in shared memory).
+    if (g->last_key >= 2 && st[kStPushRounds] > 0) {
+        const size_t per_warp = ((g->n * 4 + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
+        const double per_round = double(st[kStPushTraversals]) / double(st[kStPushRounds]);
+        g->push_hint[g->last_key] =
+            (per_warp > size_t(112) * 1024 && per_round * 40.0 > double(g->m)) ? 2 : 1;
+    }
+}
+
 int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials) {
     const int key = form_key(cfg);
     const size_t rs = cfg.precision == TGTP_PRECISION_FP64 ? 8 : 4;
     const bool mixed = cfg.precision == TGTP_PRECISION_MIXED;
-    const size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) +
-                            (mixed ? 8 * g->n : 0) + kAccBytes;
+    size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
+    if (mixed && per_warp + 8 * g->n <= size_t(112) * 1024) per_warp += 8 * g->n;
     std::vector<uint16_t> cand;
     for (int w : {1, 2})
         if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(kLayoutSmem | w));
@@ -2570,7 +2601,8 @@ tgtp_status tgtp_run(tgtp_graph* g, const tgtp_config* cfg, float* host_scores) 
         finish_run(g);
         TGTP_CUDA(cudaMemcpyAsync(host_scores, g->out.ptr, sizeof(float) * g->m,
                                   cudaMemcpyDeviceToHost, g->stream));
-        TGTP_CUDA(cudaStreamSynchronize(g->stream));
+        unsigned long long st[kStCount];
+        aesc_read_stats(g, st);  // synchronises; keeps the push hint current
     });
 }
 
@@ -2579,13 +2611,8 @@ tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out) {
         if (!g || !out) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
         if (!g->have_run) fail(TGTP_ERR_INVALID_ARGUMENT, "no run on this graph yet");
         finish_run(g);
-        unsigned long long stripes[kStCount * kStStripes];
-        TGTP_CUDA(cudaMemcpyAsync(stripes, g->stats.ptr, sizeof(stripes), cudaMemcpyDeviceToHost,
-                                  g->stream));
-        TGTP_CUDA(cudaStreamSynchronize(g->stream));
         unsigned long long st[kStCount] = {};
-        for (int c = 0; c < kStStripes; ++c)
-            for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
+        aesc_read_stats(g, st);
         out->push_rounds = st[kStPushRounds];
         out->push_vertices = st[kStPushVertices];
         out->push_traversals = st[kStPushTraversals];

@@ -112,7 +112,12 @@ tgtp_status tgtp_batch_create(tgtp_graph* const* graphs, const tgtp_config* conf
             if (tune_trials > 0) aesc_tune(graphs[i], configs[i], device_scores[i], tune_trials);
             aesc_run(graphs[i], configs[i], device_scores[i]);
         }
-        for (uint32_t i = 0; i < count; ++i) aesc_check_flags(graphs[i]);
+        for (uint32_t i = 0; i < count; ++i) {
+            aesc_check_flags(graphs[i]);
+            unsigned long long st[32];
+            aesc_read_stats(graphs[i], st);  // measures which push suits a mixed run
+            if (tune_trials <= 0) aesc_run(graphs[i], configs[i], device_scores[i]);
+        }
         auto b = std::make_unique<tgtp_batch>();
         b->origin = stream_acquire();
         for (uint32_t i = 0; i < count; ++i) {

@@ -171,6 +171,10 @@ struct tgtp_graph {
     tgtp::DeviceBuffer row_list;  // rows with a slot of tau > 1 (their marks follow the counters)
     uint16_t src_layout[4] = {0, 0, 0, 0};  // tuned source-kernel layout per form (0 = default)
     int batch_refs = 0;  // live batches whose CUDA graph points at this handle's buffers
+    int last_key = -1;   // form of the last run (see form_key in aesc.cu)
+    // mixed form, per vector storage: 2 when the last completed run's frontiers were large enough
+    // for the multi-source block push to pay off, 1 when not, 0 unknown
+    uint8_t push_hint[4] = {0, 0, 0, 0};
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
@@ -197,5 +201,8 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores);
 int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials);
 // Error flags of the handle's last run as a failure (synchronises the handle's stream).
 void aesc_check_flags(tgtp_graph* g);
+// Run counters of the last run summed over their stripes (synchronises the handle's stream); also
+// records from them which push of the mixed form suits this graph (push_hint).
+void aesc_read_stats(tgtp_graph* g, unsigned long long* st);
 void graph_prepare(tgtp_graph* g);
 }  // namespace tgtp
