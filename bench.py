@@ -31,6 +31,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from tgtp_b200 import replicas  # noqa: E402
+
 METRIC = "walk transitions/s; AESC edges/s at ε, mixed vs FP64 on 1 B200; % HBM peak"
 N_VERT, N_EDGES, EXPONENT, OMEGA, GAMMA, EPS = 4039, 88234, 2.5, 128, 10, 0.05
 WORKLOAD = ("tgtp AESC, plain FP64 form: Chung-Lu n=4039 E=88234 exp 2.5 (LCC), omega=128, "
@@ -195,12 +197,11 @@ def run_batch_workload(args):
     from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, Batch, PRECISION_FP64,
                                 PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64)
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank, world, local = replicas.rank_info()
+    torch.cuda.set_device(local)
     os.environ.setdefault("TGTP_KERNEL_DEADLINE_S", "300")
     t0 = time.perf_counter()
-    work = synth.config5_graphs(5 + rank, 64)
+    work = synth.config5_graphs(replicas.workload_seed(5, rank), 64)
     graphs = []
     for g, eps in work:
         vals, vecs, _, _, _ = eigenprep_gpu.compute(g.n, g.u, g.v, OMEGA, seed=1, tol=1e-6,
@@ -259,19 +260,18 @@ def run_batch_workload(args):
     dev = np.concatenate([np.abs(o.cpu().numpy().astype(np.float64) - f) / np.abs(f)
                           for o, f in zip(outs, fp64)])
     b.free()
-    t = torch.tensor([batch_s, sum(fp64_secs)], dtype=torch.float64, device="cuda")
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    batch_s, fp64_total = float(t[0]), float(t[1])
+    batch_s, fp64_total = replicas.slowest([batch_s, sum(fp64_secs)], device="cuda")
     if rank == 0:
         hbm, peak_kind = peaks()
         line = {
-            "metric": METRIC, "value": world * E / batch_s, "unit": "edges/s", "n_gpus": world,
+            "metric": METRIC, "value": replicas.job_rate(E, batch_s, world), "unit": "edges/s",
+            "n_gpus": world,
             "steps": steps, "warmup": 1, "ms_per_step": batch_s * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed form, bf16 vectors)",
             "data": "synthetic (64 seeded graphs + GPU eigen prep)",
@@ -280,7 +280,8 @@ def run_batch_workload(args):
                                    "from {0.05, 0.01, 0.005}, omega=128, gamma=10",
                        "undirected_edges": E, "vertices": sum(g.n for g, _, _ in graphs),
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
-            "fp64_one_by_one": {"edges_per_s": world * E / fp64_total, "seconds": fp64_total,
+            "fp64_one_by_one": {"edges_per_s": replicas.job_rate(E, fp64_total, world),
+                                "seconds": fp64_total,
                                 "slowest": sorted(((round(s, 3), g.name, eps) for s, (g, eps, _)
                                                    in zip(fp64_secs, graphs)), reverse=True)[:3]},
             "mixed_one_by_one": {"edges_per_s": E / sum(mixed_secs), "seconds": sum(mixed_secs)},
@@ -350,9 +351,7 @@ def main():
     import numpy as np
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = replicas.rank_info()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -365,7 +364,7 @@ def main():
                                 PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64, load_eigens_txt,
                                 saba_count)
 
-    seed = 1 + rank
+    seed = replicas.workload_seed(1, rank)
     root = tempfile.mkdtemp(prefix=f"tgtp_bench_r{rank}_")
     g, gpath, epath = make_inputs(seed, os.path.join(root, "cl4039"))
     idx, adj = g.csr()
@@ -431,11 +430,8 @@ def main():
                         "kernel_ms": {k: v[1] / v[0] for k, v in kx.items()},
                         "max_rel_dev_vs_fp64": float(dev.max())}
 
-    dev_ms = torch.tensor([ms64 / args.steps], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(dev_ms, op=torch.distributed.ReduceOp.MAX)
-    ms_step = float(dev_ms.item())
-    value = world * E / (ms_step * 1e-3)
+    (ms_step,) = replicas.slowest([ms64 / args.steps], device="cuda")
+    value = replicas.job_rate(E, ms_step * 1e-3, world)
 
     # ---- e2e: public API with pinned host buffers ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -461,10 +457,8 @@ def main():
     for _ in range(args.e2e_steps):
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * E / float(e2e_t.item())
+    (e2e_slowest,) = replicas.slowest([e2e_s], device="cuda")
+    e2e_value = replicas.job_rate(E, e2e_slowest, world)
     # parity guard on the e2e output (same scores as the resident run)
     ok_e2e = bool(np.array_equal(h_out.numpy(), out64.cpu().numpy()))
 
