@@ -1,0 +1,86 @@
+"""Seeded workloads from the command line, for profiling and quick checks on a GPU.
+
+    python -m tgtp_b200.workloads aesc --graph config1 --eps 0.005 --precision mixed [--repeat 2]
+    python -m tgtp_b200.workloads saba --graph config3 --depth 5 --walks 2048 [--repeat 2]
+
+Graphs: config1 (Chung-Lu n=4,039, 88,234 edges, exponent 2.5), config3 (R-MAT scale 18, edge
+factor 16, a=0.57), sparse5k (Chung-Lu n=5,000, 12,000 edges, exponent 2.1).  AESC inputs get
+128 eigenpairs from the scipy eigen prep.  Prints one line per run: seconds and work counters.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import tempfile
+import time
+
+
+def _graph(name: str):
+    from . import synth
+
+    if name == "config1":
+        return synth.config1_graph(1)
+    if name == "config3":
+        return synth.config3_graph(1)
+    if name == "sparse5k":
+        return synth.chung_lu(5000, 12000, 2.1, 7)
+    raise SystemExit(f"unknown graph {name}")
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("kind", choices=["aesc", "saba"])
+    ap.add_argument("--graph", default="config1")
+    ap.add_argument("--eps", type=float, default=0.05)
+    ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="fp64")
+    ap.add_argument("--vectors", choices=["f32", "bf16"], default="f32")
+    ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--walks", type=int, default=2048)
+    ap.add_argument("--repeat", type=int, default=1)
+    args = ap.parse_args(argv)
+
+    from . import aesc as A
+
+    g = _graph(args.graph)
+    idx, adj = g.csr()
+    dg = A.AESCGraph.from_csr(idx, adj)
+    if args.kind == "saba":
+        for _ in range(args.repeat):
+            t = time.perf_counter()
+            _, vc, cs, fb = A.saba_count(dg, args.depth, args.walks, counters=False)
+            print(f"saba {args.graph} d{args.depth} w{args.walks}: {time.perf_counter() - t:.4f} s "
+                  f"visit_count {vc} checksum {cs} fallback_bouquets {fb}", flush=True)
+        dg.free()
+        return 0
+    from . import eigenprep
+
+    d = tempfile.mkdtemp(prefix="tgtp_workload_")
+    synth_path = os.path.join(d, "graph.txt")
+    from . import synth
+
+    synth.write_graph_txt(g, synth_path)
+    path = eigenprep.eigenprep_folder(d, 128)
+    values, v32, v64 = A.load_eigens_txt(path, g.n, 128)
+    prec = {"fp32": A.PRECISION_FP32, "fp64": A.PRECISION_FP64, "mixed": A.PRECISION_MIXED}
+    if args.precision == "fp64":
+        dg.upload_eigens(values, v64, A.VEC_F64)
+    elif args.vectors == "bf16":
+        dg.upload_eigens(values, v32, A.VEC_BF16)
+    else:
+        dg.upload_eigens(values, v32, A.VEC_F32)
+    cfg = A.AESCConfig(args.eps, precision=prec[args.precision],
+                       vec_dtype=A.VEC_BF16 if args.vectors == "bf16" else A.VEC_F32)
+    a = A.AESC(dg, cfg)
+    for _ in range(args.repeat):
+        t = time.perf_counter()
+        a.tgtp()
+        st = a.stats()
+        print(f"aesc {args.graph} eps {args.eps} {args.precision}: {time.perf_counter() - t:.4f} s "
+              f"rounds {st['push_rounds']} traversals {st['push_traversals']} "
+              f"walk_hops {st['walk_hops']}", flush=True)
+    dg.free()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
