@@ -9,7 +9,7 @@
 //
 // Errors are thrown as std::runtime_error / std::invalid_argument with the reference's messages.
 // The arithmetic form is AESCConfig::precision (default: the reference's own FP32 arithmetic) or,
-// for the CLIs, the TGTP_PRECISION environment variable (fp32 | fp64).
+// for the CLIs, the TGTP_PRECISION environment variable (fp32 | fp64 | mixed).
 #pragma once
 
 #include <cstdint>

@@ -1,6 +1,6 @@
 // Drop-in for the reference's `tgtp` executable (src/main.cpp:8-50): same argv, same validation
 // and messages, same output (m raw native-endian float32 scores in CSR order), exit 0 / 1 with
-// "tgtp: <msg>" on stderr.  Arithmetic form: TGTP_PRECISION=fp32 (default) | fp64.
+// "tgtp: <msg>" on stderr.  Arithmetic form: TGTP_PRECISION=fp32 (default) | fp64 | mixed.
 #include <cmath>
 #include <climits>
 #include <filesystem>
