@@ -24,6 +24,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 #include <type_traits>
 
@@ -2087,12 +2088,26 @@ void grow(tgtp_graph* g, DeviceBuffer& b, size_t want) {
     b.reserve(want);
 }
 
-// Weight tables of the split tau kernel for the configured omega, cached on the graph: row 0 =
-// 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) from the same FP64 power chain as the
+// Weight tables of the split tau kernel for the configured omega, cached on the graph and formed
+// on the device: row 0 = 1 + lambda_i, row k + 1 = lambda_i^(2(k+1)) / (1 - lambda_i) from the
 // parity forms' eigen_t_1 table, zero at the indices the reference leaves out (0 and omega - 1)
 // and in the padding of each row to a multiple of 64.  FP64 for the FP64 form, FP32 (rounded from
 // the FP64 values) for the mixed form.
 uint32_t split_pad(uint32_t omega) { return (omega + 63u) & ~63u; }
+
+__global__ void split_tables_kernel(const double* __restrict__ onep, const double* __restrict__ onem,
+                                    const double* __restrict__ etab, uint32_t stride,
+                                    uint32_t omega, uint32_t wpad, uint32_t total,
+                                    double* __restrict__ t64, float* __restrict__ t32) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= total) return;
+    const uint32_t k = x / wpad, i = x % wpad;
+    double v = 0.0;
+    if (i >= 1 && i + 1 < omega)
+        v = k == 0 ? onep[i] : __ddiv_rn(etab[size_t(k - 1) * stride + i], onem[i]);
+    t64[x] = v;
+    t32[x] = __double2float_rn(v);
+}
 
 void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
     if (g->split_omega == omega && g->wtab32.ptr && g->wtab64.ptr) return;
@@ -2100,26 +2115,13 @@ void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
         fail(TGTP_ERR_INVALID_ARGUMENT,
              "this graph belongs to a live batch built for another omega; free the batch first");
     const uint32_t rows = 1 + kTauTableRows, wpad = split_pad(omega);
-    std::vector<double> t(size_t(rows) * wpad, 0.0);
-    for (uint32_t i = 1; i + 1 < omega; ++i) {
-        const double lam = g->values[i];
-        const double sq = lam * lam, onem = 1 - lam;
-        t[i] = 1 + lam;
-        double e = sq;
-        for (uint32_t k = 0; k < uint32_t(kTauTableRows); ++k) {
-            t[size_t(k + 1) * wpad + i] = e / onem;
-            e *= sq;
-        }
-    }
-    std::vector<float> tf(t.size());
-    for (size_t i = 0; i < t.size(); ++i) tf[i] = float(t[i]);
-    g->wtab64.reserve(sizeof(double) * t.size());
-    g->wtab32.reserve(sizeof(float) * tf.size());
-    TGTP_CUDA(cudaMemcpyAsync(g->wtab64.ptr, t.data(), sizeof(double) * t.size(),
-                              cudaMemcpyHostToDevice, g->stream));
-    TGTP_CUDA(cudaMemcpyAsync(g->wtab32.ptr, tf.data(), sizeof(float) * tf.size(),
-                              cudaMemcpyHostToDevice, g->stream));
-    TGTP_CUDA(cudaStreamSynchronize(g->stream));
+    g->wtab64.reserve(sizeof(double) * rows * wpad);
+    g->wtab32.reserve(sizeof(float) * rows * wpad);
+    const uint32_t total = rows * wpad;
+    split_tables_kernel<<<(total + 255) / 256, 256, 0, g->stream>>>(
+        g->onep.as<double>(), g->onem.as<double>(), g->etab.as<double>(), g->omega, omega, wpad,
+        total, g->wtab64.as<double>(), g->wtab32.as<float>());
+    TGTP_LAUNCH_CHECK("split_tables_kernel");
     g->split_omega = omega;
 }
 
@@ -2497,10 +2499,17 @@ void aesc_check_flags(tgtp_graph* g) {
 }
 
 void aesc_read_stats(tgtp_graph* g, unsigned long long* st) {
-    unsigned long long stripes[kStCount * kStStripes];
+    // the striped counters and the work words behind them, in one copy
+    unsigned long long stripes[kStCount * kStStripes + 2];
     TGTP_CUDA(cudaMemcpyAsync(stripes, g->stats.ptr, sizeof(stripes), cudaMemcpyDeviceToHost,
                               g->stream));
     TGTP_CUDA(cudaStreamSynchronize(g->stream));
+    unsigned work[4];
+    std::memcpy(work, stripes + kStCount * kStStripes, sizeof(work));
+    if (work[1] & kErrDeadline)
+        fail(TGTP_ERR_TIMEOUT, "device time budget exceeded (TGTP_KERNEL_DEADLINE_S)");
+    if (work[1] & kErrWalkCount)
+        fail(TGTP_ERR_UNSUPPORTED, "a walk count exceeds the 32-bit walk grid");
     for (int i = 0; i < kStCount; ++i) st[i] = 0;
     for (int c = 0; c < kStStripes; ++c)
         for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
@@ -2598,11 +2607,10 @@ tgtp_status tgtp_run(tgtp_graph* g, const tgtp_config* cfg, float* host_scores) 
         if (!g || !cfg || !host_scores) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
         g->out.reserve(sizeof(float) * (g->m + 1));
         aesc_run(g, *cfg, g->out.as<float>());
-        finish_run(g);
         TGTP_CUDA(cudaMemcpyAsync(host_scores, g->out.ptr, sizeof(float) * g->m,
                                   cudaMemcpyDeviceToHost, g->stream));
         unsigned long long st[kStCount];
-        aesc_read_stats(g, st);  // synchronises; keeps the push hint current
+        aesc_read_stats(g, st);  // synchronises once for scores, counters and error flags
     });
 }
 

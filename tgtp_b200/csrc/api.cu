@@ -68,9 +68,14 @@ void* cache_alloc(size_t bytes, size_t* granted) {
     return p;
 }
 
+// Set while a graph whose stream has been synchronised releases its buffers: no work can still use
+// them, so the per-block device synchronisation is skipped.
+thread_local bool g_release_quiet = false;
+
 void cache_free(void* p, size_t granted) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        (!g_release_quiet && cudaDeviceSynchronize() != cudaSuccess)) {
         (void)cudaGetLastError();
         cudaFree(p);
         return;
@@ -201,6 +206,45 @@ __global__ void row_of_kernel(const uint32_t* __restrict__ idx, uint64_t n, uint
     }
 }
 
+// Per-slot checks of an uploaded CSR (after row_of, which needs only monotone offsets): neighbour
+// ids below n (bit 0), rows sorted ascending (bit 1), a repeated neighbour (bit 2); and the degree
+// summary (max, min, vertices with a nonzero degree).  info = {flags, max, min, active}.
+__global__ void validate_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
+                                const uint32_t* __restrict__ row_of, uint64_t n, uint64_t m,
+                                unsigned* __restrict__ info) {
+    unsigned flags = 0, mx = 0, mn = 0xffffffffu, act = 0;
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < m;
+         q += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t a = adj[q];
+        if (a >= n) flags |= 1u;
+        if (q > idx[row_of[q]]) {
+            const uint32_t b = adj[q - 1];
+            if (a < b) flags |= 2u;
+            if (a == b) flags |= 4u;
+        }
+    }
+    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+         v += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t d = idx[v + 1] - idx[v];
+        mx = max(mx, d);
+        mn = min(mn, d);
+        act += d != 0;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        flags |= __shfl_xor_sync(kFullMask, flags, o);
+        mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+        mn = min(mn, __shfl_xor_sync(kFullMask, mn, o));
+        act += __shfl_xor_sync(kFullMask, act, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (flags) atomicOr(info, flags);
+        atomicMax(info + 1, mx);
+        atomicMin(info + 2, mn);
+        if (act) atomicAdd(info + 3, act);
+    }
+}
+
 // rev[pos] = lower_bound(row v, u) for slot (u, v): the slot src/aesc.h:207-209 and :541-542 address.
 // sym_src[q] = 1 + max{pos : rev[pos] == q}: the slot whose value lands in rev_preds[q] last
 // (src/aesc.h:538-545 writes rows in order, so the largest pos wins).
@@ -296,6 +340,25 @@ __global__ void forward_fill_kernel(const uint32_t* __restrict__ adj,
     }
 }
 
+// 1 + lambda_i, 1 - lambda_i and eigen_t_1 = lambda_i^2, lambda_i^4, ... by repeated
+// multiplication (double, and its float cast), one thread per eigen index.
+__global__ void eigen_tables_kernel(const double* __restrict__ values, uint32_t omega, int rows,
+                                    double* __restrict__ onep, double* __restrict__ onem,
+                                    double* __restrict__ tab, float* __restrict__ tabf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= omega) return;
+    const double v = values[i];
+    onep[i] = __dadd_rn(1.0, v);
+    onem[i] = __dsub_rn(1.0, v);
+    const double sq = __dmul_rn(v, v);
+    double e = sq;
+    for (int k = 0; k < rows; ++k) {
+        tab[size_t(k) * omega + i] = e;
+        tabf[size_t(k) * omega + i] = __double2float_rn(e);
+        e = __dmul_rn(e, sq);
+    }
+}
+
 __global__ void f64_to_storage_kernel(const double* __restrict__ in, uint64_t count,
                                       float* __restrict__ out_f32, __nv_bfloat16* __restrict__ out_bf16) {
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
@@ -328,11 +391,40 @@ void graph_prepare(tgtp_graph* g) {
     g->row_of.reserve(sizeof(uint32_t) * (m + 1));
     g->rev.reserve(sizeof(uint32_t) * (m + 1));
     g->sym_src.reserve(sizeof(uint32_t) * (m + 1));
+    // first the maps that read neighbour ids only as values, the checks, the forward counts
+    DeviceBuffer cnt, lbp;
+    cnt.reserve(sizeof(uint32_t) * (n + 8));
+    lbp.reserve(sizeof(uint32_t) * (n + 1));
+    auto* c = cnt.as<uint32_t>();
+    unsigned* info = c + n + 1;  // forward total, then {flags, max, min, active}
+    const unsigned init[5] = {0u, 0u, 0u, 0xffffffffu, 0u};
+    TGTP_CUDA(cudaMemcpyAsync(info, init, sizeof(init), cudaMemcpyHostToDevice, s));
     degree_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, n, g->deg.as<uint32_t>());
     TGTP_LAUNCH_CHECK("degree_kernel");
     if (m) {
         row_of_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(idx, n, m, g->row_of.as<uint32_t>());
         TGTP_LAUNCH_CHECK("row_of_kernel");
+    }
+    validate_kernel<<<grid_for(std::max(n, m), g->num_sms), 256, 0, s>>>(
+        idx, adj, g->row_of.as<uint32_t>(), n, m, info + 1);
+    TGTP_LAUNCH_CHECK("validate_kernel");
+    forward_count_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c,
+                                                                 lbp.as<uint32_t>());
+    TGTP_LAUNCH_CHECK("forward_count_kernel");
+    scan_kernel<<<1, 1024, 0, s>>>(c, n, info);
+    TGTP_LAUNCH_CHECK("scan_kernel");
+    unsigned h[5] = {0, 0, 0, 0, 0};
+    TGTP_CUDA(cudaMemcpyAsync(h, info, sizeof(h), cudaMemcpyDeviceToHost, s));
+    TGTP_CUDA(cudaStreamSynchronize(s));
+    if (h[1] & 1u) fail(TGTP_ERR_INVALID_ARGUMENT, "neighbour id out of range");
+    if (h[1] & 2u) fail(TGTP_ERR_INVALID_ARGUMENT, "rows must be sorted");
+    g->has_multi_edges = (h[1] & 4u) != 0;
+    g->max_degree = h[2];
+    g->min_degree = h[3];
+    g->num_active = h[4];
+    const uint32_t total = h[0];
+    // then the maps that index by neighbour id
+    if (m) {
         TGTP_CUDA(cudaMemsetAsync(g->sym_src.ptr, 0, sizeof(uint32_t) * m, s));
         rev_kernel<<<grid_for(m, g->num_sms), 256, 0, s>>>(idx, adj, g->row_of.as<uint32_t>(), m,
                                                            g->rev.as<uint32_t>(),
@@ -343,19 +435,6 @@ void graph_prepare(tgtp_graph* g) {
                                                             g->adjd.as<uint2>());
         TGTP_LAUNCH_CHECK("adjd_kernel");
     }
-    // forward slot list
-    DeviceBuffer cnt, lbp;
-    cnt.reserve(sizeof(uint32_t) * (n + 2));
-    lbp.reserve(sizeof(uint32_t) * (n + 1));
-    auto* c = cnt.as<uint32_t>();
-    forward_count_kernel<<<grid_for(n, g->num_sms), 256, 0, s>>>(idx, adj, n, c,
-                                                                 lbp.as<uint32_t>());
-    TGTP_LAUNCH_CHECK("forward_count_kernel");
-    scan_kernel<<<1, 1024, 0, s>>>(c, n, c + n + 1);
-    TGTP_LAUNCH_CHECK("scan_kernel");
-    uint32_t total = 0;
-    TGTP_CUDA(cudaMemcpyAsync(&total, c + n + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    TGTP_CUDA(cudaStreamSynchronize(s));
     g->num_forward = total;
     g->forward.reserve(sizeof(uint32_t) * (total + 1));
     g->fedge.reserve(sizeof(uint4) * (total + 1));
@@ -364,7 +443,7 @@ void graph_prepare(tgtp_graph* g) {
             adj, g->row_of.as<uint32_t>(), g->rev.as<uint32_t>(), m, c, lbp.as<uint32_t>(),
             g->forward.as<uint32_t>(), g->fedge.as<uint4>());
     TGTP_LAUNCH_CHECK("forward_fill_kernel");
-    TGTP_CUDA(cudaStreamSynchronize(s));
+    // the temporaries go back to the cache when this returns (their release waits for the device)
 }
 
 }  // namespace tgtp
@@ -398,27 +477,10 @@ tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t
         auto g = std::make_unique<tgtp_graph>();
         g->n = n;
         g->m = m;
-        uint32_t maxd = 0, mind = 0xffffffffu;
-        uint64_t active = 0;
-        bool multi = false;
-        for (uint64_t v = 0; v < n; ++v) {
+        // monotone offsets here (the device maps rely on them); neighbour ranges, row order,
+        // repeated neighbours and the degree summary are checked on the device (graph_prepare)
+        for (uint64_t v = 0; v < n; ++v)
             if (idx[v + 1] < idx[v]) fail(TGTP_ERR_INVALID_ARGUMENT, "row offsets decrease");
-            const uint32_t d = idx[v + 1] - idx[v];
-            maxd = std::max(maxd, d);
-            mind = std::min(mind, d);
-            active += d != 0;
-            for (uint32_t p = idx[v]; p < idx[v + 1]; ++p) {
-                if (adj[p] >= n) fail(TGTP_ERR_INVALID_ARGUMENT, "neighbour id out of range");
-                if (p > idx[v]) {
-                    if (adj[p] < adj[p - 1]) fail(TGTP_ERR_INVALID_ARGUMENT, "rows must be sorted");
-                    if (adj[p] == adj[p - 1]) multi = true;
-                }
-            }
-        }
-        g->max_degree = maxd;
-        g->min_degree = mind;
-        g->num_active = active;
-        g->has_multi_edges = multi;
         TGTP_CUDA(cudaGetDevice(&g->device));
         TGTP_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
         g->own_stream = stream_acquire();
@@ -437,9 +499,15 @@ tgtp_status tgtp_graph_upload(const uint32_t* idx, const uint32_t* adj, uint64_t
 
 tgtp_status tgtp_graph_free(tgtp_graph* g) {
     return guarded([&] {
-        if (g && g->batch_refs > 0)
+        if (!g) return;
+        if (g->batch_refs > 0)
             fail(TGTP_ERR_INVALID_ARGUMENT, "this graph belongs to a live batch; free the batch first");
+        // every use of the graph's buffers was ordered on its stream: one synchronisation of that
+        // stream covers the release of all of them
+        TGTP_CUDA(cudaStreamSynchronize(g->stream));
+        g_release_quiet = true;
         delete g;
+        g_release_quiet = false;
     });
 }
 
@@ -489,33 +557,17 @@ tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* 
         TGTP_CUDA(cudaMemcpyAsync(g->d_values.ptr, values, sizeof(double) * omega,
                                   cudaMemcpyHostToDevice, s));
         // tau-bound tables: onep/onem per eigen index, and eigen_t_1 after k multiplications
-        // (src/aesc.h:174-176, :190, :201-203), in the reference's exact sequence of roundings.
+        // (src/aesc.h:174-176, :190, :201-203), in the reference's exact sequence of roundings,
+        // formed on the device from the uploaded values
         constexpr int kRows = 64;
-        std::vector<double> onep(omega), onem(omega), tab(size_t(kRows) * omega);
-        std::vector<float> tabf(size_t(kRows) * omega);
-        for (uint32_t i = 0; i < omega; ++i) {
-            onep[i] = 1 + values[i];
-            onem[i] = 1 - values[i];
-            const double sq = values[i] * values[i];
-            double e = sq;
-            for (int k = 0; k < kRows; ++k) {
-                tab[size_t(k) * omega + i] = e;
-                tabf[size_t(k) * omega + i] = float(e);
-                e *= sq;
-            }
-        }
         g->onep.reserve(sizeof(double) * omega);
         g->onem.reserve(sizeof(double) * omega);
-        g->etab.reserve(sizeof(double) * tab.size());
-        g->etab_f.reserve(sizeof(float) * tabf.size());
-        TGTP_CUDA(cudaMemcpyAsync(g->onep.ptr, onep.data(), sizeof(double) * omega,
-                                  cudaMemcpyHostToDevice, s));
-        TGTP_CUDA(cudaMemcpyAsync(g->onem.ptr, onem.data(), sizeof(double) * omega,
-                                  cudaMemcpyHostToDevice, s));
-        TGTP_CUDA(cudaMemcpyAsync(g->etab.ptr, tab.data(), sizeof(double) * tab.size(),
-                                  cudaMemcpyHostToDevice, s));
-        TGTP_CUDA(cudaMemcpyAsync(g->etab_f.ptr, tabf.data(), sizeof(float) * tabf.size(),
-                                  cudaMemcpyHostToDevice, s));
+        g->etab.reserve(sizeof(double) * kRows * omega);
+        g->etab_f.reserve(sizeof(float) * kRows * omega);
+        eigen_tables_kernel<<<(omega + 127) / 128, 128, 0, s>>>(
+            g->d_values.as<double>(), omega, kRows, g->onep.as<double>(), g->onem.as<double>(),
+            g->etab.as<double>(), g->etab_f.as<float>());
+        TGTP_LAUNCH_CHECK("eigen_tables_kernel");
         const unsigned blocks = grid_for(count, g->num_sms);
         if (dtype == TGTP_VEC_F32) {
             g->vec_f32.reserve(sizeof(float) * count);
