@@ -91,3 +91,47 @@ def test_saba_zero_walks_and_zero_depth(cuda_device):
         counts, visits, checksum, _ = saba_count(g, d, w)
         assert visits == 0 and checksum == 0 and not counts.any()
     g.free()
+
+
+def test_saba_rmat18_counters_match_oracle_at_full_graph_size(cuda_device, oracle_lib):
+    """The R-MAT scale-18 walk graph (174,015 vertices, 7.6M slots) with 8 walks of depth 5 per
+    vertex: every counter equal to the oracle's."""
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    g = synth.config3_graph(1)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, _, _ = saba_count(dg, 5, 8)
+    want = oracle_lib.saba(idx, adj, 5, 8)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    assert visits == g.n * 8 * 5
+    dg.free()
+
+
+def test_saba_rmat18_benchmark_size_two_kernels_agree(cuda_device):
+    """The benchmark configuration (depth 5, 2,048 walks per vertex, 1.78e9 transitions): the
+    degree-renumbered kernel of saba_count and the plain kernel behind saba_count_static give the
+    same visit count, checksum and fallback count, and visit_count = n * W * D exactly."""
+    import ctypes as C
+
+    import torch
+
+    from tgtp_b200 import _lib, synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    g = synth.config3_graph(1)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    _, visits, checksum, fallbacks = saba_count(dg, 5, 2048, counters=False)
+    assert visits == g.n * 2048 * 5
+    d_idx = torch.from_numpy(idx.astype(np.int32)).cuda()
+    d_adj = torch.from_numpy(adj.astype(np.int32)).cuda()
+    torch.cuda.synchronize()
+    res = _lib.SabaResult()
+    _lib.check(_lib.lib().saba_count_static(C.c_void_p(d_idx.data_ptr()),
+                                            C.c_void_p(d_adj.data_ptr()), g.n, 5, 2048, None,
+                                            C.byref(res)))
+    assert (int(res.visit_count), int(res.checksum), int(res.fallback_bouquets)) == (
+        visits, checksum, fallbacks)
+    dg.free()
