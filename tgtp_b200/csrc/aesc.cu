@@ -727,6 +727,7 @@ struct SourceParams {
     Real* pvec_g;         // n per warp (global tier)
     unsigned long long* rbuf;  // n per warp: frontier residuals in fixed point (Jacobi push)
     unsigned long long* fx_g;  // n per warp: fixed-point accumulators (Jacobi push, global tier)
+    unsigned char* wclean;     // per warp: 1 = its HBM vectors are all zero (left so by its last run)
     unsigned char* vis_g; // vis_stride per warp (global tier)
     size_t vis_stride;
     size_t smem_per_warp;
@@ -1196,7 +1197,10 @@ source_kernel(SourceParams<Real, Acc> p) {
         fx = JACOBI ? p.fx_g + gw * size_t(n) : nullptr;
         acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
-    bool cleared = false;  // pvec and flags are zeroed once, before the warp's first source
+    // pvec and flags are zeroed once, before the warp's first source, unless the warp's last run
+    // (same layout, HBM tier) left them zero: every source resets what it touched
+    bool cleared = !SMEM && p.wclean[gw] != 0;
+    bool dirty = false;  // a source stopped midway (time-out): its vectors are not zero
     uint32_t* qa = p.qbuf + gw * 2 * size_t(n);
     uint32_t* qb = qa + n;
     WalkItem* items = p.items + gw * size_t(p.max_degree);
@@ -1647,6 +1651,7 @@ source_kernel(SourceParams<Real, Acc> p) {
         }
         if (timed_out) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);
+            dirty = true;
             break;
         }
         if (!p.pre) st_rounds += ell;  // PrePush rounds are counted by push_block_kernel
@@ -1989,6 +1994,7 @@ source_kernel(SourceParams<Real, Acc> p) {
         __syncwarp();
         lap(7);
     }
+    if (!SMEM && lane == 0) p.wclean[gw] = (cleared && !dirty) ? 1 : 0;
     if (lane == 0) {
         stat_add(p.stats, kStPushRounds, st_rounds);
         stat_add(p.stats, kStPushVertices, st_pv);
@@ -2356,6 +2362,19 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.vis_g = use_smem ? nullptr : base;
     base += visg_bytes;
     p.fx_g = fxg_bytes ? reinterpret_cast<unsigned long long*>(base) : nullptr;
+    // the per-warp "vectors are zero" marks hold only for the same carving of the same scratch
+    {
+        const uint64_t sig[5] = {uint64_t(key) | (uint64_t(use_smem) << 8) | (uint64_t(wpb) << 16),
+                                 blocks, uint64_t(n),
+                                 uint64_t(reinterpret_cast<uintptr_t>(g->scratch.ptr)),
+                                 uint64_t(g->scratch.bytes)};
+        grow(g, g->wclean, warps + 16);
+        if (std::memcmp(sig, g->wclean_sig, sizeof(sig)) != 0) {
+            TGTP_CUDA(cudaMemsetAsync(g->wclean.ptr, 0, warps + 16, s));
+            std::memcpy(g->wclean_sig, sig, sizeof(sig));
+        }
+        p.wclean = g->wclean.as<unsigned char>();
+    }
     p.vis_stride = vis_bytes;
     p.smem_per_warp = per_warp;
     p.max_degree = uint32_t(maxd);

@@ -170,6 +170,8 @@ struct tgtp_graph {
     uint32_t split_omega = 0;
     tgtp::DeviceBuffer row_list;  // rows with a slot of tau > 1 (their marks follow the counters)
     uint16_t src_layout[4] = {0, 0, 0, 0};  // tuned source-kernel layout per form (0 = default)
+    tgtp::DeviceBuffer wclean;  // per warp of the source kernel: HBM vectors left all zero
+    uint64_t wclean_sig[5] = {0, 0, 0, 0, 0};  // the scratch carving those marks belong to
     int batch_refs = 0;  // live batches whose CUDA graph points at this handle's buffers
     int last_key = -1;   // form of the last run (see form_key in aesc.cu)
     // mixed form, per vector storage: 2 when the last completed run's frontiers were large enough
