@@ -87,3 +87,16 @@ def test_oracle_saba_rejects_partial_bouquets(oracle_lib, tgtp_lib):
     idx, adj = _csr_from_graph(os.path.join(GOLDEN, "saba", "cl300.graph.txt"))
     with pytest.raises(ValueError):
         oracle_lib.saba(idx, adj, 3, 12)
+
+
+def test_sampled_exact_matches_dense_exact():
+    """The sampled-edge oracle (block PCG) against the dense solve on a graph both can handle."""
+    from oracle import exact_sc
+    from tgtp_b200 import synth
+
+    g = synth.chung_lu(800, 4000, 2.3, 3)
+    idx, adj = g.csr()
+    exact = exact_sc.exact_scores(idx, adj)
+    slots = np.random.default_rng(0).choice(len(adj), 200, replace=False)
+    got = exact_sc.sampled_scores(idx, adj, slots)
+    assert np.max(np.abs(got - exact[slots])) < 1e-9

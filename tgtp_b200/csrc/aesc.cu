@@ -561,28 +561,155 @@ tau_sums_kernel(const uint4* __restrict__ fedge, uint64_t num_forward, const Vec
     }
 }
 
-// Stage 1b: the bound per edge, one lane per edge (src/aesc.h:181-207): tau_0 from lambda_1, then
-// tau' from delta_k while t <= tau' < tau (t += 2).  Edges that need a further delta sweep are
-// served four at a time by the warp's 8-lane groups.  Writes tau to both slots and marks the two
-// rows when tau > 1.
+// The bound of one edge per lane (src/aesc.h:181-207): tau_0 from lambda_1, then tau' from
+// delta_k while t <= tau' < tau (t += 2).  Edges that need a further delta sweep are served four
+// at a time by the warp's 8-lane groups.  Writes tau to both slots and marks the two rows when
+// tau > 1.  All 32 lanes of the warp call it together; act says whether the lane holds an edge.
 template <class Vec>
-__global__ void __launch_bounds__(256)
-tau_bound_kernel(const uint4* __restrict__ fedge, const uint32_t* __restrict__ deg,
-                 uint64_t num_forward, const double2* __restrict__ sums,
-                 const Vec* __restrict__ vec, uint32_t stride, uint32_t omega,
-                 const typename Split<Vec>::Part* __restrict__ wtab, uint32_t wpad,
-                 const double* __restrict__ etabd, const double* __restrict__ onem,
-                 double eps_half, uint64_t m, TauConst c, int* __restrict__ taus, RowMarks rm,
-                 unsigned long long* __restrict__ stats) {
+struct BoundArgs {
+    const uint32_t* deg;
+    const Vec* vec;
+    uint32_t stride, omega;
+    const typename Split<Vec>::Part* wtab;
+    uint32_t wpad;
+    const double* etabd;
+    const double* onem;
+    double eps_half, mdbl;
+    TauConst c;
+    int* taus;
+    RowMarks rm;
+};
+
+template <class Vec>
+__device__ __forceinline__ void bound_lanes(const BoundArgs<Vec>& A, bool act, uint4 rec, double2 sm,
+                                            unsigned long long& iters,
+                                            unsigned long long& ambiguous) {
     using Part = typename Split<Vec>::Part;
     constexpr bool kF64 = std::is_same<Vec, double>::value;
     constexpr uint32_t P = Split<Vec>::P, C = 8 * P;
     const uint32_t lane = threadIdx.x & 31, grp = lane >> 3, sl = lane & 7;
+    const bool vec_ok = A.stride % P == 0;
+    const double inv_b1 = 1.0 / A.c.b1, inv_b2 = 1.0 / A.c.b2;
+    uint32_t du = 1, dv = 1;
+    if (act) {
+        du = __ldg(A.deg + rec.x);
+        dv = __ldg(A.deg + rec.y);
+    }
+    const double inv1 = 1.0 / double(du), inv2 = 1.0 / double(dv);
+    auto bound = [&](double one_m_lam2, double b, double inv_b, double dl, double up) {
+        if constexpr (kF64) {
+            return get_tau<double>(du, dv, A.eps_half, one_m_lam2, b, dl, up, ambiguous);
+        } else {
+            return get_tau_mixed(inv1, inv2, A.eps_half, one_m_lam2, inv_b, dl, up);
+        }
+    };
+    int tau = 0, t = 1;
+    uint32_t k = 1;
+    bool need = false;
+    double ups = 0;
+    if (act) {
+        ups = kF64 ? __ddiv_rn(sm.x, A.mdbl) : sm.x / A.mdbl;
+        const double del = kF64 ? __ddiv_rn(sm.y, A.mdbl) : sm.y / A.mdbl;
+        tau = bound(A.c.one_m_l1sq, A.c.b1, inv_b1, 0.0, 0.0);
+        ++iters;
+        const int tp = bound(A.c.one_m_l2sq, A.c.b2, inv_b2, del, ups);
+        if (t <= tp && tp < tau) {
+            tau = tp;
+            t += 2;
+            need = true;
+        }
+    }
+    // further delta sweeps (:191-204), four edges at a time
+    unsigned nb;
+    while ((nb = __ballot_sync(kFullMask, need)) != 0) {
+        int sel[4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            sel[g] = nb ? __ffs(nb) - 1 : -1;
+            if (nb) nb &= nb - 1;
+        }
+        const uint32_t src_lane = sel[grp] < 0 ? 0u : uint32_t(sel[grp]);
+        const uint32_t gu = __shfl_sync(kFullMask, rec.x, src_lane);
+        const uint32_t gv = __shfl_sync(kFullMask, rec.y, src_lane);
+        const uint32_t gk = __shfl_sync(kFullMask, k, src_lane);
+        Part s2 = Part(0);
+        if (sel[grp] >= 0) {
+            const Vec* ur = A.vec + size_t(gu) * A.stride;
+            const Vec* vr = A.vec + size_t(gv) * A.stride;
+            if (gk < uint32_t(kTauTableRows)) {
+                split_pass<Vec, 1>(ur, vr, A.omega, vec_ok, sl, nullptr,
+                                   A.wtab + size_t(gk + 1) * A.wpad, s2, s2);
+            } else {
+                for (uint32_t i0 = sl * P; i0 < A.omega; i0 += C) {
+                    Part xu[P], xv[P];
+                    load_piece(ur, i0, A.omega, vec_ok, xu);
+                    load_piece(vr, i0, A.omega, vec_ok, xv);
+#pragma unroll
+                    for (uint32_t j = 0; j < P; ++j)
+                        s2 = split_fma(split_sub(xu[j], xv[j]),
+                                       split_weight<Part>(A.wtab, A.wpad, gk, i0 + j, A.omega,
+                                                          A.etabd, A.stride, A.onem),
+                                       s2);
+                }
+            }
+        }
+        const double dsum = split_reduce(s2);
+        double mine = 0.0;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const double r = __shfl_sync(kFullMask, dsum, g * 8);
+            if (sel[g] == int(lane)) mine = r;
+        }
+        bool served = false;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) served |= sel[g] == int(lane);
+        if (served) {
+            const double del = kF64 ? __ddiv_rn(mine, A.mdbl) : mine / A.mdbl;
+            ++iters;
+            const int tp = bound(A.c.one_m_l2sq, A.c.b2, inv_b2, del, ups);
+            if (t <= tp && tp < tau) {
+                tau = tp;
+                t += 2;
+                ++k;
+            } else {
+                need = false;
+            }
+        }
+    }
+    if (act) {
+        A.taus[rec.z] = tau;
+        A.taus[rec.w] = tau;
+        if (tau > 1) {
+            mark_row(A.rm, rec.x);
+            mark_row(A.rm, rec.y);
+        }
+    }
+}
+
+__device__ __forceinline__ void flush_tau_stats(unsigned long long iters, unsigned long long ambiguous,
+                                                unsigned long long* stats) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        iters += __shfl_xor_sync(kFullMask, iters, o);
+        ambiguous += __shfl_xor_sync(kFullMask, ambiguous, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        stat_add(stats, kStTauIters, iters);
+        stat_add(stats, kStTauAmbiguous, ambiguous);
+    }
+}
+
+// Stage 1b: the bound per edge, one lane per edge (a variant that evaluated the bounds inside the
+// gather kernel, 32 edges per warp at a time, measured slower: the bound's FP64 chains then sit on
+// the gather's critical path).
+template <class Vec>
+__global__ void __launch_bounds__(256)
+tau_bound_kernel(const uint4* __restrict__ fedge, uint64_t num_forward,
+                 const double2* __restrict__ sums, BoundArgs<Vec> A,
+                 unsigned long long* __restrict__ stats) {
+    const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-    const bool vec_ok = stride % P == 0;
-    const double mdbl = double(m);
-    const double inv_b1 = 1.0 / c.b1, inv_b2 = 1.0 / c.b2;
     unsigned long long iters = 0, ambiguous = 0;
     pdl_launch_dependents();
     pdl_wait();  // the sums of tau_sums_kernel
@@ -591,112 +718,13 @@ tau_bound_kernel(const uint4* __restrict__ fedge, const uint32_t* __restrict__ d
         const bool act = e < num_forward;
         uint4 rec = make_uint4(0, 0, 0, 0);
         double2 sm = make_double2(0.0, 0.0);
-        uint32_t du = 1, dv = 1;
         if (act) {
             rec = __ldg(fedge + e);
             sm = sums[e];
-            du = __ldg(deg + rec.x);
-            dv = __ldg(deg + rec.y);
         }
-        const double inv1 = 1.0 / double(du), inv2 = 1.0 / double(dv);
-        auto bound = [&](double one_m_lam2, double b, double inv_b, double dl, double up) {
-            if constexpr (kF64) {
-                return get_tau<double>(du, dv, eps_half, one_m_lam2, b, dl, up, ambiguous);
-            } else {
-                return get_tau_mixed(inv1, inv2, eps_half, one_m_lam2, inv_b, dl, up);
-            }
-        };
-        int tau = 0, t = 1;
-        uint32_t k = 1;
-        bool need = false;
-        double ups = 0;
-        if (act) {
-            ups = kF64 ? __ddiv_rn(sm.x, mdbl) : sm.x / mdbl;
-            const double del = kF64 ? __ddiv_rn(sm.y, mdbl) : sm.y / mdbl;
-            tau = bound(c.one_m_l1sq, c.b1, inv_b1, 0.0, 0.0);
-            ++iters;
-            const int tp = bound(c.one_m_l2sq, c.b2, inv_b2, del, ups);
-            if (t <= tp && tp < tau) {
-                tau = tp;
-                t += 2;
-                need = true;
-            }
-        }
-        // further delta sweeps (:191-204), four edges at a time
-        unsigned nb;
-        while ((nb = __ballot_sync(kFullMask, need)) != 0) {
-            int sel[4];
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                sel[g] = nb ? __ffs(nb) - 1 : -1;
-                if (nb) nb &= nb - 1;
-            }
-            const uint32_t src_lane = sel[grp] < 0 ? 0u : uint32_t(sel[grp]);
-            const uint32_t gu = __shfl_sync(kFullMask, rec.x, src_lane);
-            const uint32_t gv = __shfl_sync(kFullMask, rec.y, src_lane);
-            const uint32_t gk = __shfl_sync(kFullMask, k, src_lane);
-            Part s2 = Part(0);
-            if (sel[grp] >= 0) {
-                const Vec* ur = vec + size_t(gu) * stride;
-                const Vec* vr = vec + size_t(gv) * stride;
-                if (gk < uint32_t(kTauTableRows)) {
-                    split_pass<Vec, 1>(ur, vr, omega, vec_ok, sl, nullptr,
-                                       wtab + size_t(gk + 1) * wpad, s2, s2);
-                } else {
-                    for (uint32_t i0 = sl * P; i0 < omega; i0 += C) {
-                        Part xu[P], xv[P];
-                        load_piece(ur, i0, omega, vec_ok, xu);
-                        load_piece(vr, i0, omega, vec_ok, xv);
-#pragma unroll
-                        for (uint32_t j = 0; j < P; ++j)
-                            s2 = split_fma(split_sub(xu[j], xv[j]),
-                                           split_weight<Part>(wtab, wpad, gk, i0 + j, omega, etabd,
-                                                              stride, onem),
-                                           s2);
-                    }
-                }
-            }
-            const double dsum = split_reduce(s2);
-            double mine = 0.0;
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                const double r = __shfl_sync(kFullMask, dsum, g * 8);
-                if (sel[g] == int(lane)) mine = r;
-            }
-            bool served = false;
-#pragma unroll
-            for (int g = 0; g < 4; ++g) served |= sel[g] == int(lane);
-            if (served) {
-                const double del = kF64 ? __ddiv_rn(mine, mdbl) : mine / mdbl;
-                ++iters;
-                const int tp = bound(c.one_m_l2sq, c.b2, inv_b2, del, ups);
-                if (t <= tp && tp < tau) {
-                    tau = tp;
-                    t += 2;
-                    ++k;
-                } else {
-                    need = false;
-                }
-            }
-        }
-        if (act) {
-            taus[rec.z] = tau;
-            taus[rec.w] = tau;
-            if (tau > 1) {
-                mark_row(rm, rec.x);
-                mark_row(rm, rec.y);
-            }
-        }
+        bound_lanes<Vec>(A, act, rec, sm, iters, ambiguous);
     }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        iters += __shfl_xor_sync(kFullMask, iters, o);
-        ambiguous += __shfl_xor_sync(kFullMask, ambiguous, o);
-    }
-    if (lane == 0) {
-        stat_add(stats, kStTauIters, iters);
-        stat_add(stats, kStTauAmbiguous, ambiguous);
-    }
+    flush_tau_stats(iters, ambiguous, stats);
 }
 
 // ---- stage 2: per-source push, edge bound and walks -----------------------------------------------
@@ -2249,26 +2277,41 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
                                                              : (const Part*)g->wtab32.ptr;
         const uint32_t wpad = split_pad(omega);
         const size_t ssmem = 2 * sizeof(Part) * wpad;
-        const int per_sm =
-            blocks_per_sm(reinterpret_cast<const void*>(tau_sums_kernel<Vec>), 256, ssmem);
-        if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel");
-        grow(g, g->tau_sums, sizeof(double2) * (g->num_forward + 1));
-        const uint64_t need = (g->num_forward + 63) / 64;  // 64 edges per block and step
-        const unsigned blocks = unsigned(std::max<uint64_t>(
-            1, std::min<uint64_t>(need, uint64_t(g->num_sms) * per_sm)));
+        BoundArgs<Vec> ba;
+        ba.deg = g->deg.as<uint32_t>();
+        ba.vec = vec;
+        ba.stride = g->omega;
+        ba.omega = omega;
+        ba.wtab = wtab;
+        ba.wpad = wpad;
+        ba.etabd = g->etab.as<double>();
+        ba.onem = g->onem.as<double>();
+        ba.eps_half = cfg.epsilon / 2.0;
+        ba.mdbl = double(m);
+        ba.c = c;
+        ba.taus = g->taus.as<int>();
+        ba.rm = rm;
         {
-            ScopedKernel k(g->prof, s, "tau_sums");
-            launch(tau_sums_kernel<Vec>, blocks, 256, ssmem, s, false,
-                g->fedge.as<uint4>(), g->num_forward, vec, g->omega, omega, wtab, wpad,
-                g->tau_sums.as<double2>());
-            TGTP_LAUNCH_CHECK("tau_sums_kernel");
+            const int per_sm =
+                blocks_per_sm(reinterpret_cast<const void*>(tau_sums_kernel<Vec>), 256, ssmem);
+            if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "omega too large for the tau kernel");
+            grow(g, g->tau_sums, sizeof(double2) * (g->num_forward + 1));
+            const uint64_t need = (g->num_forward + 63) / 64;  // 64 edges per block and step
+            const unsigned blocks = unsigned(std::max<uint64_t>(
+                1, std::min<uint64_t>(need, uint64_t(g->num_sms) * per_sm)));
+            {
+                ScopedKernel k(g->prof, s, "tau_sums");
+                launch(tau_sums_kernel<Vec>, blocks, 256u, ssmem, s, false,
+                    g->fedge.as<uint4>(), g->num_forward, vec, g->omega, omega, wtab, wpad,
+                    g->tau_sums.as<double2>());
+                TGTP_LAUNCH_CHECK("tau_sums_kernel");
+            }
+            ScopedKernel k(g->prof, s, "tau_bound");
+            launch(tau_bound_kernel<Vec>, grid_cap(g->num_forward, 256, g->num_sms, 8), 256u,
+                   size_t(0), s, true, g->fedge.as<uint4>(), g->num_forward,
+                   static_cast<const double2*>(g->tau_sums.as<double2>()), ba, stats);
+            TGTP_LAUNCH_CHECK("tau_bound_kernel");
         }
-        ScopedKernel k(g->prof, s, "tau_bound");
-        launch(tau_bound_kernel<Vec>, grid_cap(g->num_forward, 256, g->num_sms, 8), 256, 0, s,
-            true, g->fedge.as<uint4>(), g->deg.as<uint32_t>(), g->num_forward,
-            g->tau_sums.as<double2>(), vec, g->omega, omega, wtab, wpad, g->etab.as<double>(),
-            g->onem.as<double>(), cfg.epsilon / 2.0, m, c, g->taus.as<int>(), rm, stats);
-        TGTP_LAUNCH_CHECK("tau_bound_kernel");
     } else {
         // FP32 form: the reference's arithmetic and summation order
         const Real* vec = (const Real*)g->vec_f32.ptr;
