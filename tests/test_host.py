@@ -133,3 +133,34 @@ def test_eigenprep_pairs_are_eigenpairs_of_the_random_walk_matrix(tmp_path):
         ax = np.add.reduceat(x[adj], idx[:-1]) / deg
         assert np.max(np.abs(ax - lam * x)) < 1e-5 * np.max(np.abs(x))
     assert (tmp_path / "stat.txt").read_text().startswith("n=200\nm=")
+
+
+def test_input_cache_reuses_parsed_inputs_and_follows_the_text(tmp_path, monkeypatch, manifest, tgtp_lib):
+    """TGTP_INPUT_CACHE=1: the loaders write '<file>.tgtpcache' beside the text, later loads read
+    it and give the same arrays, and a change of the text file invalidates it."""
+    import shutil
+
+    from conftest import golden_tgtp_case
+    from tgtp_b200.aesc import load_eigens_txt, load_graph_txt
+
+    c = golden_tgtp_case(manifest, "cl300")
+    gpath = tmp_path / "graph.txt"
+    epath = tmp_path / f"sorted_eigens_{c['omega']}.txt"
+    shutil.copy(os.path.join(c["folder"], "graph.txt"), gpath)
+    shutil.copy(os.path.join(c["folder"], f"sorted_eigens_{c['omega']}.txt"), epath)
+    plain_g = load_graph_txt(str(gpath))
+    plain_e = load_eigens_txt(str(epath), c["n"], c["omega"])
+    assert not (tmp_path / "graph.txt.tgtpcache").exists()
+    monkeypatch.setenv("TGTP_INPUT_CACHE", "1")
+    for _ in range(2):  # the first call writes the caches, the second reads them
+        g = load_graph_txt(str(gpath))
+        e = load_eigens_txt(str(epath), c["n"], c["omega"])
+        assert all(np.array_equal(a, b) for a, b in zip(g, plain_g))
+        assert all(np.array_equal(a, b) for a, b in zip(e, plain_e))
+        assert (tmp_path / "graph.txt.tgtpcache").exists()
+        assert (tmp_path / f"sorted_eigens_{c['omega']}.txt.tgtpcache").exists()
+    # an edited text file is parsed again (its size and time no longer match the cache)
+    with open(gpath, "a") as f:
+        f.write(f"0 {c['n'] - 1}\n")
+    g2 = load_graph_txt(str(gpath))
+    assert int(g2[0][-1]) == int(plain_g[0][-1]) + 2  # the loader mirrors and keeps every line

@@ -9,9 +9,11 @@
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "internal.hpp"
@@ -94,6 +96,66 @@ size_t float_prefix(const char* p, const char* end) {
     return size_t(q - p);
 }
 
+
+// ---- opt-in binary cache of parsed inputs (TGTP_INPUT_CACHE=1) ----------------------------------
+// Parsing the text inputs dominates a run's wall time on large graphs (a 10^6-vertex eigen file is
+// gigabytes of decimal text).  With TGTP_INPUT_CACHE=1 the loaders keep what they parsed in
+// "<text file>.tgtpcache" beside it and reuse it while the text file's size and modification time
+// are unchanged; a cache that cannot be written (read-only folder) is skipped silently.  Off by
+// default: the reference writes nothing beside its inputs.
+struct CacheHeader {
+    char magic[8];
+    uint64_t text_size;
+    int64_t text_mtime_ns;
+    uint64_t a, b;  // graph: n, m; eigens: n, omega
+};
+
+bool cache_enabled() {
+    const char* e = std::getenv("TGTP_INPUT_CACHE");
+    return e && std::string(e) == "1";
+}
+
+bool text_stamp(const char* path, uint64_t& size, int64_t& mtime) {
+    struct stat st;
+    if (stat(path, &st) != 0) return false;
+    size = uint64_t(st.st_size);
+    mtime = int64_t(st.st_mtim.tv_sec) * 1000000000LL + int64_t(st.st_mtim.tv_nsec);
+    return true;
+}
+
+// Opens the cache of `path` if it matches the text file (magic, size, mtime); the header is read.
+FILE* cache_open(const char* path, const char* magic, CacheHeader& h) {
+    uint64_t size;
+    int64_t mtime;
+    if (!cache_enabled() || !text_stamp(path, size, mtime)) return nullptr;
+    FILE* f = std::fopen((std::string(path) + ".tgtpcache").c_str(), "rb");
+    if (!f) return nullptr;
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, magic, 8) != 0 ||
+        h.text_size != size || h.text_mtime_ns != mtime) {
+        std::fclose(f);
+        return nullptr;
+    }
+    return f;
+}
+
+// Writes the cache of `path` through a temporary file renamed into place; any failure is ignored.
+void cache_write(const char* path, const char* magic, uint64_t a, uint64_t b,
+                 const std::vector<std::pair<const void*, size_t>>& parts) {
+    CacheHeader h;
+    std::memcpy(h.magic, magic, 8);
+    h.a = a;
+    h.b = b;
+    if (!cache_enabled() || !text_stamp(path, h.text_size, h.text_mtime_ns)) return;
+    const std::string dst = std::string(path) + ".tgtpcache";
+    const std::string tmp = dst + ".tmp" + std::to_string(getpid());
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return;
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+    for (const auto& part : parts)
+        ok = ok && (part.second == 0 || std::fwrite(part.first, part.second, 1, f) == 1);
+    ok = std::fclose(f) == 0 && ok;
+    if (!ok || std::rename(tmp.c_str(), dst.c_str()) != 0) std::remove(tmp.c_str());
+}
 }  // namespace
 }  // namespace tgtp
 
@@ -108,6 +170,24 @@ tgtp_status tgtp_load_graph_txt(const char* path, uint32_t** idx_out, uint32_t**
             fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
         *idx_out = nullptr;
         *adj_out = nullptr;
+        CacheHeader ch;
+        if (FILE* cf = cache_open(path, "TGTPCSR1", ch)) {
+            const uint64_t n = ch.a, m = ch.b;
+            uint32_t* idx = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (n + 1)));
+            uint32_t* adj = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (m ? m : 1)));
+            const bool ok = idx && adj && std::fread(idx, sizeof(uint32_t), n + 1, cf) == n + 1 &&
+                            (m == 0 || std::fread(adj, sizeof(uint32_t), m, cf) == m);
+            std::fclose(cf);
+            if (ok) {
+                *idx_out = idx;
+                *adj_out = adj;
+                *n_out = n;
+                *m_out = m;
+                return;
+            }
+            std::free(idx);
+            std::free(adj);
+        }
         MappedFile f(path);
         if (!f.ok()) fail(TGTP_ERR_IO, std::string("cannot open graph: ") + path);
         const char* p = f.data;
@@ -165,6 +245,8 @@ tgtp_status tgtp_load_graph_txt(const char* path, uint32_t** idx_out, uint32_t**
             adj[fill[dst[e]]++] = src[e];
         }
         for (uint64_t v = 0; v < n; ++v) std::sort(adj + idx[v], adj + idx[v + 1]);
+        cache_write(path, "TGTPCSR1", n, m,
+                    {{idx, sizeof(uint32_t) * (n + 1)}, {adj, sizeof(uint32_t) * m}});
         *idx_out = idx;
         *adj_out = adj;
         *n_out = n;
@@ -176,8 +258,38 @@ tgtp_status tgtp_load_eigens_txt(const char* path, uint64_t n, uint32_t omega, d
                                  float* vec_f32, double* vec_f64) {
     return guarded([&] {
         if (!path || !values) fail(TGTP_ERR_INVALID_ARGUMENT, "null argument");
+        // the cache holds values, FP32 and FP64 vectors of the first `omega` pairs of an n-vertex
+        // file, parsed as below
+        CacheHeader ch;
+        if (FILE* cf = cache_open(path, "TGTPEIG1", ch)) {
+            bool ok = ch.a == n && ch.b == omega &&
+                      std::fread(values, sizeof(double), omega, cf) == omega;
+            const size_t cnt = size_t(n) * omega;
+            if (ok) {
+                if (vec_f32) ok = std::fread(vec_f32, sizeof(float), cnt, cf) == cnt;
+                else ok = fseeko(cf, off_t(sizeof(float) * cnt), SEEK_CUR) == 0;
+            }
+            if (ok && vec_f64) ok = std::fread(vec_f64, sizeof(double), cnt, cf) == cnt;
+            std::fclose(cf);
+            if (ok) return;
+        }
         MappedFile f(path);
         if (!f.ok()) fail(TGTP_ERR_IO, std::string("cannot open eigenpairs: ") + path);
+        // with the cache on, both precisions are parsed so that one cache serves every form
+        std::vector<float> keep32;
+        std::vector<double> keep64;
+        float* out32 = vec_f32;
+        double* out64 = vec_f64;
+        if (cache_enabled()) {
+            if (!out32) {
+                keep32.resize(size_t(n) * omega);
+                out32 = keep32.data();
+            }
+            if (!out64) {
+                keep64.resize(size_t(n) * omega);
+                out64 = keep64.data();
+            }
+        }
         const char* p = f.data;
         const char* end = f.data + f.size;
         std::string tok;
@@ -197,12 +309,17 @@ tgtp_status tgtp_load_eigens_txt(const char* path, uint64_t n, uint32_t omega, d
             for (uint64_t j = 0; j < n; ++j) {
                 double d;
                 float fl;
-                if (!next(vec_f64 ? &d : nullptr, vec_f32 ? &fl : (vec_f64 ? nullptr : &fl)))
+                if (!next(out64 ? &d : nullptr, out32 ? &fl : (out64 ? nullptr : &fl)))
                     fail(TGTP_ERR_IO, std::string("invalid eigenvector in ") + path);
-                if (vec_f32) vec_f32[j * omega + i] = fl;
-                if (vec_f64) vec_f64[j * omega + i] = d;
+                if (out32) out32[j * omega + i] = fl;
+                if (out64) out64[j * omega + i] = d;
             }
         }
+        if (cache_enabled())
+            cache_write(path, "TGTPEIG1", n, omega,
+                        {{values, sizeof(double) * omega},
+                         {out32, sizeof(float) * size_t(n) * omega},
+                         {out64, sizeof(double) * size_t(n) * omega}});
     });
 }
 
