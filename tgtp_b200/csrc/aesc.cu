@@ -2437,7 +2437,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         ScopedKernel k(g->prof, s, "source");
         launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
         TGTP_LAUNCH_CHECK("source_kernel");
-    } else {
+    } else if constexpr (JACOBI) {  // the block push exists for the mixed form only
         grow(g, g->block_cols, 2 * size_t(n) * kBlockCols * sizeof(float) * block_ctas);
         grow(g, g->block_pre, sizeof(PrePush) * (n + 1));
         grow(g, g->block_final, sizeof(uint32_t) * (block_ctas + 1));
@@ -2448,7 +2448,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         bp.adjd = p.adjd;
         bp.n = uint32_t(n);
         bp.taus = p.taus;
-        bp.preds = reinterpret_cast<double*>(p.preds);
+        bp.preds = p.preds;
         bp.work = work;
         bp.rows = rm.list;
         bp.eps = cfg.epsilon;
