@@ -87,10 +87,14 @@ def test_mixed_matches_fp64_when_no_walks_run(cuda_device, config1_inputs):
     g.free()
 
 
+@pytest.mark.parametrize("ctas", ["0", "2"])
 @pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
-def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, monkeypatch):
+def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, ctas, monkeypatch):
     """The per-warp push and the multi-source block push sum residuals in fixed point, so the two
-    give identical scores, taus and work counters."""
+    give identical scores, taus and work counters.  ctas = 2 runs the block push with two CTAs,
+    64 sources per wave, so the larger graphs take several waves."""
+    if ctas != "0":
+        monkeypatch.setenv("TGTP_BLOCK_CTAS", ctas)
     from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_MIXED, VEC_BF16, VEC_F32
 
     c = golden_tgtp_case(manifest, name)

@@ -2250,11 +2250,15 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
     else block_mode = JACOBI && g->push_hint[key] == 2;
     g->last_key = key;
+    // CTAs of the block push: one per SM, within a 24 GB budget for their residual blocks
+    // (TGTP_BLOCK_CTAS lowers the count, e.g. to exercise many waves on small graphs)
     uint32_t block_ctas = uint32_t(g->num_sms);
     {
         const size_t per_cta = 2 * size_t(n) * kBlockCols * sizeof(float);
         const size_t budget = size_t(24) << 30;
         block_ctas = uint32_t(std::max<size_t>(1, std::min<size_t>(block_ctas, budget / per_cta)));
+        if (const char* e = std::getenv("TGTP_BLOCK_CTAS"))
+            block_ctas = std::max(1u, std::min(block_ctas, uint32_t(std::atoi(e))));
     }
     const uint32_t waves =
         block_mode ? uint32_t((n + uint64_t(block_ctas) * kBlockCols - 1) / (uint64_t(block_ctas) * kBlockCols))
