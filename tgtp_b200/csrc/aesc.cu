@@ -1,22 +1,29 @@
 // tgtp() on sm_100a: the TGT+ approximate edge spanning centrality of src/aesc.h:113-551.
 //
-// Stages (one launch each, all on the graph's stream):
-//   1. tau_kernel         per undirected edge (u <= v): the omega-eigenvector walk-length bound
-//                         (calculate_taus, :164-216), written to both CSR slots.
-//   2. source_kernel      persistent warps, one source at a time per warp (dynamic queue):
-//                         residual push rounds until the push/walk cost test stops them
-//                         (:456-503), the top-gamma edge bound (:414-442), the per-edge chi and
-//                         walk count (:392-412, :508-521) and the 2-way bouquet walks (:241-391),
-//                         accumulating the source's CSR row of scores (:524-525).
-//   3. symmetrize_kernel  score[q] = row[q] + row[reverse slot] (:532-550).
+// Stages (all on the graph's stream, consecutive kernels joined by programmatic dependent launch):
+//   1. tau per undirected edge (u <= v): the omega-eigenvector walk-length bound (calculate_taus,
+//      :164-216), written to both CSR slots; rows with a slot of tau > 1 are listed.
+//        FP32 form           tau_kernel<float>: the reference's sequential sums, lane per edge.
+//        FP64 / mixed forms  tau_sums_kernel (eight lanes per edge gather the rows) then
+//                            tau_bound_kernel (lane per edge evaluates the bound).
+//   2. the listed sources: push rounds until the push/walk cost test stops them (:456-503), the
+//      top-gamma edge bound (:414-442), the per-edge chi and walk count (:392-412, :508-521) and
+//      the 2-way bouquet walks (:241-391), accumulating each source's CSR row (:524-525).
+//        source_kernel       persistent warps, one source at a time per warp;
+//        push_block_kernel   mixed form on large graphs: the push of 32 sources per CTA as a
+//                            pull product, then source_kernel for the rest (PrePush mode).
+//   3. finish_kernel: score[q] = row[q] + row[reverse slot] (:532-550), with the rows of unlisted
+//      sources (every tau <= 1: one push round, no walks) in closed form.
 //
-// The parity forms (FP32 = the reference's own arithmetic, FP64 = every float held in double)
+// The parity forms (FP32 = the reference's own arithmetic, FP64 = every real held in double)
 // keep the reference's evaluation order wherever a rounding depends on it:
 //   * the push of one source is sequential over its frontier, in discovery order; the lanes of the
 //     warp share one frontier vertex's adjacency (distinct neighbours, so their updates commute);
-//   * float sums run in the reference's order (tau dot products per edge in index order, walk
-//     lanes per bouquet lane in bouquet order, the eight lanes summed 0..7);
-//   * every operation is a correctly rounded intrinsic, never contracted into an FMA.
+//   * float sums run in the reference's order (walk lanes per bouquet lane in bouquet order, the
+//     eight lanes summed 0..7; the FP32 form's tau dot products per edge in index order, the FP64
+//     form's in its fixed eight-way split);
+//   * every operation is a correctly rounded intrinsic, never contracted into an FMA except the
+//     FP64 form's tau terms, which are defined as fused multiply-adds.
 // Max/min/integer reductions are order-free and run across lanes.
 #include <cuda_bf16.h>
 
@@ -26,13 +33,12 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
-#include <type_traits>
-
 #include <map>
-
-#include <cub/device/device_radix_sort.cuh>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -337,7 +343,7 @@ tau_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
     }
 }
 
-// ---- stage 1 (mixed form): tau with lane-parallel, compensated FP32 projections ---------------
+// ---- stage 1 helpers of the mixed form: compensated FP32 sums, FP64 bound, fixed-point residuals
 // d_i^2 = (x_u[i] - x_v[i])^2 and the weighted terms d_i^2 (1 + lambda_i) and
 // d_i^2 lambda_i^(2(k+1)) / (1 - lambda_i) are formed in FP32 from F32 or BF16 eigenvectors; the
 // bound itself (get_tau: logs, ceil, odd rounding, the delta iteration) is evaluated in FP64.
