@@ -126,3 +126,20 @@ def test_invalid_arguments_are_rejected(manifest, cuda_device):
         g.upload_eigens(np.array([1.0, 0.5]), np.zeros(8, np.float32))
         AESC(g, AESCConfig(0.05, omega=2)).tgtp()
     g.free()
+
+
+def test_fp64_bulk_copy_tau_gives_the_same_bits(manifest, cuda_device, oracle_lib, monkeypatch):
+    """TGTP_TAU_BULK=1 moves the eigen rows into shared memory with cp.async.bulk before summing;
+    the sums, and so the scores, are the same bits as the FP64 oracle's."""
+    from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_FP64
+
+    monkeypatch.setenv("TGTP_TAU_BULK", "1")
+    c = golden_tgtp_case(manifest, "cl300")
+    g = _device_graph(c, fp64=True)
+    for run in c["runs"]:
+        got = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"],
+                                 precision=PRECISION_FP64)).tgtp()
+        ora = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], run["epsilon"],
+                              gamma=run["gamma"], fp64=True)
+        assert np.array_equal(got.view(np.uint32), ora.view(np.uint32)), run
+    g.free()
