@@ -1142,6 +1142,7 @@ struct PushBlockParams {
     float* cols;           // per CTA: two n x S blocks
     uint32_t* final_buf;   // per CTA: the block that holds the final columns
     PrePush* pre;          // per list entry
+    bool bits;             // the row bitmasks fit in shared memory
     unsigned long long* stats;
     uint64_t budget_ns;
 };
@@ -1149,6 +1150,9 @@ struct PushBlockParams {
 __global__ void __launch_bounds__(1024, 1)
 push_block_kernel(PushBlockParams p) {
     constexpr int S = kBlockCols;
+    // With p.bits: one bit per row, set when a running column of the row is nonzero (cur and nxt
+    // rounds); the pull skips the 128-byte reads of neighbour rows whose bit is clear.
+    extern __shared__ uint32_t s_bits[];
     __shared__ uint32_t s_src[S], s_rb[S], s_ds[S], s_support[S], s_ell[S];
     __shared__ unsigned long long s_picost[S];
     __shared__ unsigned s_max[S], s_min[S];  // float bits of non-negative residuals
@@ -1170,6 +1174,11 @@ push_block_kernel(PushBlockParams p) {
     // round 1 in closed form: the frontier {src} pushes 1 / deg(u) to every neighbour u
     for (size_t i = threadIdx.x; i < size_t(n) * S / 4; i += blockDim.x)
         reinterpret_cast<float4*>(A)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t words = (n + 31) / 32;
+    uint32_t* bcur = s_bits;
+    uint32_t* bnxt = s_bits + words;
+    if (p.bits)
+        for (uint32_t i = threadIdx.x; i < 2 * words; i += blockDim.x) s_bits[i] = 0u;
     if (threadIdx.x < S) {
         const uint32_t j = threadIdx.x;
         s_active[j] = j < cnt;
@@ -1191,6 +1200,7 @@ push_block_kernel(PushBlockParams p) {
             const uint2 a = __ldg(p.adjd + rb + o);
             const float pu = from_fixed(kFixOne, a.y);
             A[size_t(a.x) * S + j] = pu;
+            if (p.bits) atomicOr(bcur + (a.x >> 5), 1u << (a.x & 31));
             pc += a.y;
             mx = fmaxf(mx, pu);
             mn = fminf(mn, pu);
@@ -1273,6 +1283,8 @@ push_block_kernel(PushBlockParams p) {
             s_min[threadIdx.x] = __float_as_uint(1.f);
             s_support[threadIdx.x] = 0;
         }
+        if (p.bits)
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
         __syncthreads();
         const bool run = lane < cnt && s_active[lane];
         unsigned long long pc = 0;
@@ -1283,16 +1295,25 @@ push_block_kernel(PushBlockParams p) {
             unsigned long long acc = 0;
             for (uint32_t c = 0; c < ud; c += 32) {
                 const uint32_t nb = c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u;
-                const uint32_t k = min(32u, ud - c);
+                // neighbours whose running columns are all zero add nothing: with the bitmask they
+                // are dropped, and the live ones compacted into lanes 0 .. popc(live) - 1 (the
+                // fixed-point sum does not depend on the order)
+                const bool in = c + lane < ud;
+                const unsigned live = __ballot_sync(
+                    kFullMask, in && (!p.bits || ((bcur[nb >> 5] >> (nb & 31)) & 1u)));
+                const uint32_t nth = lane < uint32_t(__popc(live)) ? __fns(live, 0, int(lane) + 1) : 0u;
+                const uint32_t packed = __shfl_sync(kFullMask, nb, nth);
+                const uint32_t k = __popc(live);
                 uint32_t t = 0;
                 for (; t + 4 <= k; t += 4) {
-                    const float x0 = cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane];
-                    const float x1 = cur[size_t(__shfl_sync(kFullMask, nb, t + 1)) * S + lane];
-                    const float x2 = cur[size_t(__shfl_sync(kFullMask, nb, t + 2)) * S + lane];
-                    const float x3 = cur[size_t(__shfl_sync(kFullMask, nb, t + 3)) * S + lane];
+                    const float x0 = cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane];
+                    const float x1 = cur[size_t(__shfl_sync(kFullMask, packed, t + 1)) * S + lane];
+                    const float x2 = cur[size_t(__shfl_sync(kFullMask, packed, t + 2)) * S + lane];
+                    const float x3 = cur[size_t(__shfl_sync(kFullMask, packed, t + 3)) * S + lane];
                     acc += to_fixed(x0) + to_fixed(x1) + to_fixed(x2) + to_fixed(x3);
                 }
-                for (; t < k; ++t) acc += to_fixed(cur[size_t(__shfl_sync(kFullMask, nb, t)) * S + lane]);
+                for (; t < k; ++t)
+                    acc += to_fixed(cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane]);
             }
             float r = cur[size_t(u) * S + lane];
             if (run) {
@@ -1304,6 +1325,8 @@ push_block_kernel(PushBlockParams p) {
                     mn = fminf(mn, r);
                 }
             }
+            if (p.bits && __any_sync(kFullMask, run && r > 0.f) && lane == 0)
+                atomicOr(bnxt + (u >> 5), 1u << (u & 31));
             nxt[size_t(u) * S + lane] = r;
         }
         if (run) {
@@ -1329,6 +1352,9 @@ push_block_kernel(PushBlockParams p) {
         float* t = cur;
         cur = nxt;
         nxt = t;
+        uint32_t* tb = bcur;
+        bcur = bnxt;
+        bnxt = tb;
         fin ^= 1u;
     }
     if (threadIdx.x == 0) p.final_buf[blockIdx.x] = fin;
@@ -2660,6 +2686,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         bp.pre = g->block_pre.as<PrePush>();
         bp.stats = stats;
         bp.budget_ns = p.budget_ns;
+        // two row bitmasks in shared memory while they fit beside the kernel's static 1.3 KB
+        const size_t bits_bytes = 2 * sizeof(uint32_t) * ((size_t(n) + 31) / 32);
+        bp.bits = bits_bytes <= size_t(200) * 1024;
+        const size_t bsm = bp.bits ? bits_bytes : 0;
+        if (bsm) (void)blocks_per_sm(reinterpret_cast<const void*>(push_block_kernel), 1024, bsm);
         p.pre = bp.pre;
         p.pre_cols = bp.cols;
         p.pre_final = bp.final_buf;
@@ -2688,7 +2719,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             bp.base = w * block_ctas * kBlockCols;
             {
                 ScopedKernel k(g->prof, s, "push_block");
-                launch(push_block_kernel, block_ctas, 1024u, size_t(0), s, true, bp);
+                launch(push_block_kernel, block_ctas, 1024u, bsm, s, true, bp);
                 TGTP_LAUNCH_CHECK("push_block_kernel");
             }
             p.claim = claims + w;
