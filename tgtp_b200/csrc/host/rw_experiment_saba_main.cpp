@@ -1,8 +1,14 @@
-// Drop-in for the reference's `rw_experiment_saba` (src/rw_experiment_saba.cpp:147-247): same argv,
-// same results/rw/saba_<dataset>_d<D>_w<W>.txt keys and the same TSV row.  t_load_s covers reading
-// graph.txt and placing the CSR on the device; t_rw_s covers zeroing the counters, every walk and
-// the visit_count / checksum reduction (the reference's timed scope).  The counters are exact
-// integers; visit_count and checksum are printed as doubles as the reference prints them.
+// Drop-in for the reference's `rw_experiment_saba` (src/rw_experiment_saba.cpp:147-247).
+//
+//   rw_experiment_saba <datasets_folder> <dataset> <depth> <n_walks> [threads]
+//
+// Counts the visits of n_walks SABA walks of `depth` hops from every vertex of
+// <datasets_folder>/<dataset>/graph.txt on the GPU, writes results/rw/saba_<dataset>_d<D>_w<W>.txt
+// ("key value" lines) and prints the same values as one TSV row.  t_load_s covers reading graph.txt
+// and placing the CSR on the device; t_rw_s covers zeroing the counters, every walk and the
+// visit_count / checksum reduction (the reference's timed scope).  The counters are exact integers;
+// visit_count and checksum are printed as doubles, as the reference prints them.  `threads` is
+// echoed for format compatibility.
 #include <chrono>
 #include <cstdint>
 #include <cstdlib>
@@ -11,73 +17,88 @@
 #include <iostream>
 #include <string>
 
+#include "cli.hpp"
 #include "tgtp_aesc.hpp"
 
-namespace fs = std::filesystem;
-static const char* const VARIANT = "saba";
+namespace {
+
+constexpr const char* kVariant = "saba";
+
+struct Walks {
+    std::string folder, dataset;
+    size_t depth = 0, n_walks = 0;
+    int threads = 1;
+};
+
+double seconds_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+void count_walks(const Walks& w) {
+    using clock = std::chrono::steady_clock;
+    tgtp_b200::Graph g;
+    const auto t_start = clock::now();
+    g.load_txt((std::filesystem::path(w.folder) / w.dataset / "graph.txt").string());
+    const auto t_loaded = clock::now();
+    saba_result res{};
+    tgtp_b200::check(saba_count(g.handle, uint32_t(w.depth), uint32_t(w.n_walks), nullptr, &res));
+    const auto t_walked = clock::now();
+    const size_t n = g.n, m = g.m;
+    g.free();
+
+    const double t_load = seconds_between(t_start, t_loaded);
+    const double t_rw = seconds_between(t_loaded, t_walked);
+    const double walks = double(n) * double(w.n_walks) * double(w.depth);
+    tgtp_cli::Record rec;
+    rec.add("variant", kVariant)
+        .add("dataset", w.dataset)
+        .add("depth", w.depth)
+        .add("n_walks", w.n_walks)
+        .add("threads", w.threads)
+        .add("n_vertices", n)
+        .add("n_edges", m)
+        .add("t_load_s", t_load)
+        .add("t_rw_s", t_rw)
+        .add("total_s", seconds_between(t_start, t_walked))
+        .add("total_walks", walks)
+        .add("walks_per_sec", t_rw > 0 ? walks / t_rw : 0.0)
+        .add("visit_count", double(res.visit_count))
+        .add("checksum", double(res.checksum));
+
+    const std::filesystem::path dir = "results/rw";
+    std::filesystem::create_directories(dir);
+    const std::string file = std::string(kVariant) + "_" + w.dataset + "_d" + std::to_string(w.depth) +
+                             "_w" + std::to_string(w.n_walks) + ".txt";
+    {
+        std::ofstream out(dir / file);
+        rec.write_lines(out);
+    }
+    rec.write_row(std::cout);
+}
+
+}  // namespace
 
 int main(int argc, char** argv) {
     if (argc < 5) {
         std::cerr << "Usage: " << argv[0] << " <datasets_folder> <dataset> <depth> <n_walks> [threads]\n";
         return 1;
     }
-    const std::string folder = argv[1];
-    const std::string dataset = argv[2];
-    const size_t depth = std::strtoull(argv[3], nullptr, 10);
-    const size_t n_walks = std::strtoull(argv[4], nullptr, 10);
-    if (n_walks % 8 != 0 || n_walks > UINT32_MAX) {
+    Walks w;
+    w.folder = argv[1];
+    w.dataset = argv[2];
+    w.depth = std::strtoull(argv[3], nullptr, 10);
+    w.n_walks = std::strtoull(argv[4], nullptr, 10);
+    // the walk grid splits the 32-bit seed range into n_walks steps, one bouquet per 8 walks
+    if (w.n_walks % 8 != 0 || w.n_walks > UINT32_MAX) {
         std::cerr << "n_walks must be a multiple of 8 within the 32-bit grid domain\n";
         return 1;
     }
-    int threads = (argc > 5) ? std::atoi(argv[5]) : 1;
-    if (threads < 1) threads = 1;
+    w.threads = argc > 5 ? std::atoi(argv[5]) : 1;
+    if (w.threads < 1) w.threads = 1;
     try {
-        const fs::path graph_path = fs::path(folder) / dataset / "graph.txt";
-        tgtp_b200::Graph g;
-        auto t0 = std::chrono::high_resolution_clock::now();
-        g.load_txt(graph_path.string());
-        auto t1 = std::chrono::high_resolution_clock::now();
-        const double t_load = std::chrono::duration<double>(t1 - t0).count();
-        const size_t n = g.n, m = g.m;
-
-        auto t2 = std::chrono::high_resolution_clock::now();
-        saba_result res{};
-        tgtp_b200::check(saba_count(g.handle, uint32_t(depth), uint32_t(n_walks), nullptr, &res));
-        auto t3 = std::chrono::high_resolution_clock::now();
-        const double t_rw = std::chrono::duration<double>(t3 - t2).count();
-        const double total = std::chrono::duration<double>(t3 - t0).count();
-        const double total_walks = (double)n * (double)n_walks * (double)depth;
-        const double walks_per_sec = (t_rw > 0.0) ? (total_walks / t_rw) : 0.0;
-        const double visit_count = double(res.visit_count);
-        const double checksum = double(res.checksum);
-        g.free();
-
-        fs::create_directories("results/rw");
-        const std::string resfile = "results/rw/" + std::string(VARIANT) + "_" + dataset + "_d" +
-                                    std::to_string(depth) + "_w" + std::to_string(n_walks) + ".txt";
-        {
-            std::ofstream out(resfile);
-            out << "variant " << VARIANT << "\n";
-            out << "dataset " << dataset << "\n";
-            out << "depth " << depth << "\n";
-            out << "n_walks " << n_walks << "\n";
-            out << "threads " << threads << "\n";
-            out << "n_vertices " << n << "\n";
-            out << "n_edges " << m << "\n";
-            out << "t_load_s " << t_load << "\n";
-            out << "t_rw_s " << t_rw << "\n";
-            out << "total_s " << total << "\n";
-            out << "total_walks " << total_walks << "\n";
-            out << "walks_per_sec " << walks_per_sec << "\n";
-            out << "visit_count " << visit_count << "\n";
-            out << "checksum " << checksum << "\n";
-        }
-        std::cout << VARIANT << "\t" << dataset << "\t" << depth << "\t" << n_walks << "\t" << threads
-                  << "\t" << n << "\t" << m << "\t" << t_load << "\t" << t_rw << "\t" << total << "\t"
-                  << total_walks << "\t" << walks_per_sec << "\t" << visit_count << "\t" << checksum
-                  << "\n";
+        count_walks(w);
     } catch (const std::exception& e) {
-        std::cerr << "rw_experiment_saba: " << e.what() << "\n";
+        std::cerr << "rw_experiment_saba: " << e.what() << '\n';
         return 1;
     }
     return 0;

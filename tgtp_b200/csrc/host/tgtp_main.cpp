@@ -1,7 +1,11 @@
-// Drop-in for the reference's `tgtp` executable (src/main.cpp:8-50): same argv, same validation
-// and messages, same output (m raw native-endian float32 scores in CSR order), exit 0 / 1 with
-// "tgtp: <msg>" on stderr.  Arithmetic form: TGTP_PRECISION=fp32 (default) | fp64 | mixed.
-#include <cmath>
+// Drop-in for the reference's `tgtp` executable (src/main.cpp:8-50).
+//
+//   tgtp <folder> <graph> <epsilon> <omega> <gamma> <outfile>
+//
+// Reads <folder>/<graph>/graph.txt and sorted_eigens_<omega>.txt, scores every CSR slot on the GPU
+// and writes the m scores as raw native-endian float32 in CSR order.  Exit 0, or 1 with
+// "tgtp: <message>" on stderr (argument errors as the reference words them, tgtp_cli).
+// Arithmetic form: TGTP_PRECISION=fp32 (default, the reference's arithmetic) | fp64 | mixed.
 #include <climits>
 #include <filesystem>
 #include <fstream>
@@ -10,9 +14,62 @@
 #include <stdexcept>
 #include <string>
 
+#include "cli.hpp"
 #include "tgtp_aesc.hpp"
 
-using namespace tgtp_b200;
+namespace {
+
+struct Job {
+    std::string folder, graph, outfile;
+    double epsilon = 0;
+    int omega = 0, gamma = 0;
+};
+
+// argv[1..6]; the three numbers are read in order before any of them is range-checked.
+Job read_job(char** argv) {
+    const std::string complaint = "invalid numeric argument";
+    Job job;
+    job.folder = argv[1];
+    job.graph = argv[2];
+    job.outfile = argv[6];
+    job.epsilon = tgtp_cli::whole_number(argv[3], complaint);
+    const double omega = tgtp_cli::whole_number(argv[4], complaint);
+    const double gamma = tgtp_cli::whole_number(argv[5], complaint);
+    const bool ok = job.epsilon > 0 && job.epsilon < 1 && tgtp_cli::integral_in(omega, 2, INT_MAX) &&
+                    tgtp_cli::integral_in(gamma, 1, INT_MAX);
+    if (!ok)
+        throw std::invalid_argument("require 0 < epsilon < 1, integer omega >= 2, integer gamma >= 1");
+    job.omega = int(omega);
+    job.gamma = int(gamma);
+    return job;
+}
+
+void score(const Job& job) {
+    using namespace tgtp_b200;
+    AESCConfig config{};
+    config.strFolder = job.folder;
+    config.strGraph = job.graph;
+    config.epsilon = job.epsilon;
+    config.omega = job.omega;
+    config.gamma = job.gamma;
+    config.precision = precision_from_env();
+    const auto dir = std::filesystem::path(job.folder) / job.graph;
+    const auto eigens = dir / ("sorted_eigens_" + std::to_string(job.omega) + ".txt");
+    AESCGraph graph((dir / "graph.txt").string(), eigens.string(), size_t(job.omega), config.precision);
+    config.delta = 1.0 / double(graph.n);
+    // the output file is opened once the inputs have loaded, so an input error leaves no file
+    std::ofstream sink(job.outfile, std::ios::binary);
+    if (!sink) throw std::runtime_error("cannot open output file");
+    AESC run(graph, config);
+    const std::unique_ptr<float[]> scores(run.tgtp());
+    sink.write(reinterpret_cast<const char*>(scores.get()),
+               std::streamsize(graph.m * sizeof(float)));
+    sink.close();
+    if (!sink) throw std::runtime_error("failed to write output file");
+    graph.free();
+}
+
+}  // namespace
 
 int main(int argc, char** argv) {
     if (argc != 7) {
@@ -20,41 +77,10 @@ int main(int argc, char** argv) {
         return 1;
     }
     try {
-        AESCConfig config{};
-        config.strFolder = argv[1];
-        config.strGraph = argv[2];
-        auto number = [](const char* arg) {
-            std::size_t used;
-            double value = std::stod(arg, &used);
-            if (arg[used] != '\0' || !std::isfinite(value))
-                throw std::invalid_argument("invalid numeric argument");
-            return value;
-        };
-        config.epsilon = number(argv[3]);
-        double omega = number(argv[4]), gamma = number(argv[5]);
-        if (!(config.epsilon > 0 && config.epsilon < 1) || omega < 2 || omega > INT_MAX ||
-            omega != std::floor(omega) || gamma < 1 || gamma > INT_MAX || gamma != std::floor(gamma))
-            throw std::invalid_argument(
-                "require 0 < epsilon < 1, integer omega >= 2, integer gamma >= 1");
-        config.omega = static_cast<int>(omega);
-        config.gamma = static_cast<int>(gamma);
-        config.precision = precision_from_env();
-        auto directory = std::filesystem::path(config.strFolder) / config.strGraph;
-        AESCGraph graph((directory / "graph.txt").string(),
-                        (directory / ("sorted_eigens_" + std::to_string(config.omega) + ".txt")).string(),
-                        config.omega, config.precision);
-        config.delta = 1.0 / graph.n;
-        std::ofstream out(argv[6], std::ios::binary);
-        if (!out) throw std::runtime_error("cannot open output file");
-        AESC algo(graph, config);
-        std::unique_ptr<float[]> scores(algo.tgtp());
-        out.write(reinterpret_cast<const char*>(scores.get()), graph.m * sizeof(float));
-        out.close();
-        if (!out) throw std::runtime_error("failed to write output file");
-        graph.free();
-        return 0;
-    } catch (const std::exception& error) {
-        std::cerr << "tgtp: " << error.what() << '\n';
+        score(read_job(argv));
+    } catch (const std::exception& e) {
+        std::cerr << "tgtp: " << e.what() << '\n';
         return 1;
     }
+    return 0;
 }
