@@ -143,3 +143,35 @@ def test_fp64_bulk_copy_tau_gives_the_same_bits(manifest, cuda_device, oracle_li
                               gamma=run["gamma"], fp64=True)
         assert np.array_equal(got.view(np.uint32), ora.view(np.uint32)), run
     g.free()
+
+
+@pytest.mark.parametrize("tier", ["smem", "global"])
+def test_device_time_budget_gives_a_timeout_status_and_leaves_the_graph_usable(
+        config1_inputs, cuda_device, monkeypatch, tier):
+    """Failure detection without a GPU fault: with a device time budget of 1 ns every warp of the
+    source kernel gives up at its next check and the run returns TGTP_ERR_TIMEOUT; the next run on
+    the same graph handle (residual vectors in shared memory, or in HBM where a warp that gave up
+    left them dirty) gives the same bits and work counters as a run before the time-out."""
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, PRECISION_FP64, TgtpError, VEC_F64
+
+    monkeypatch.setenv("TGTP_PVEC_TIER", tier)
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    cfg = AESCConfig(0.005, precision=PRECISION_FP64)
+    a = AESC(g, cfg)
+    want = a.tgtp()
+    want_st = a.stats()
+    assert want_st["push_rounds"] > 0  # listed rows: the source kernel pushes
+    monkeypatch.setenv("TGTP_KERNEL_DEADLINE_S", "1e-9")
+    with pytest.raises(TgtpError) as e:
+        a.tgtp()
+    assert e.value.status == 4  # TGTP_ERR_TIMEOUT
+    monkeypatch.delenv("TGTP_KERNEL_DEADLINE_S")
+    for _ in range(2):
+        got = a.tgtp()
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        st = a.stats()
+        for k in STAT_KEYS:
+            assert st[k] == want_st[k], k
+    g.free()
