@@ -1,0 +1,45 @@
+"""bench.py's reference arm on the CPU: the reference's own `benchmark` binary timed on the host's
+cores prints one JSON line with the bench contract's keys, and under a multi-rank launch only rank
+0 does work."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT
+
+
+def _bench(*args, env=None):
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        *args], capture_output=True, text=True, cwd=ROOT, timeout=600,
+                       env=dict(os.environ, **(env or {})))
+    assert r.returncode == 0, r.stderr[-2000:]
+    return [line for line in r.stdout.splitlines() if line.startswith("{")]
+
+
+def test_reference_arm_prints_the_contract_line():
+    lines = _bench("--steps", "1", "--warmup", "3")
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    if "unavailable" in d:  # the reference binaries under oracle/_ref were not built here
+        assert set(d) == {"impl", "unavailable"}
+        return
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["unit"] == "edges/s" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
+    assert abs(d["ms_per_step"] * 1e-3 * d["value"] - 88234) < 1e-6 * 88234
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "edges/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert "workload" in d["config"]
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    assert _bench("--steps", "1", "--warmup", "3", env={"RANK": "1", "WORLD_SIZE": "2"}) == []
