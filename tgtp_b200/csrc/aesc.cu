@@ -66,6 +66,7 @@ enum StatIdx {
 // The run counters are striped over kStStripes copies (block index modulo kStStripes) so that the
 // warps of a launch do not all meet on one address; the host adds the copies up.
 constexpr int kStStripes = 32;
+static_assert(kStCount <= kRunStatSlots, "aesc_read_stats writes kStCount counters");
 
 // Forms with their own tuned source-kernel layout on a handle: FP32, FP64, MIXED over F32 rows,
 // MIXED over BF16 rows.  A layout is (kLayoutSmem if the residual vectors live in shared memory) |

@@ -114,7 +114,7 @@ tgtp_status tgtp_batch_create(tgtp_graph* const* graphs, const tgtp_config* conf
         }
         for (uint32_t i = 0; i < count; ++i) {
             aesc_check_flags(graphs[i]);
-            unsigned long long st[32];
+            unsigned long long st[kRunStatSlots];
             aesc_read_stats(graphs[i], st);  // measures which push suits a mixed run
             if (tune_trials <= 0) aesc_run(graphs[i], configs[i], device_scores[i]);
         }

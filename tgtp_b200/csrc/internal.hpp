@@ -204,7 +204,9 @@ int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int t
 // Error flags of the handle's last run as a failure (synchronises the handle's stream).
 void aesc_check_flags(tgtp_graph* g);
 // Run counters of the last run summed over their stripes (synchronises the handle's stream); also
-// records from them which push of the mixed form suits this graph (push_hint).
+// records from them which push of the mixed form suits this graph (push_hint).  st holds
+// kRunStatSlots entries (the counters fill the first ones).
+constexpr int kRunStatSlots = 32;
 void aesc_read_stats(tgtp_graph* g, unsigned long long* st);
 void graph_prepare(tgtp_graph* g);
 }  // namespace tgtp
