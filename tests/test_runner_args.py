@@ -118,3 +118,10 @@ def test_usage_lines(runners, tmp_path, name, args):
     if os.path.exists(ref):
         rrc, rout, rerr = _run(ref, args, tmp_path)
         assert (rrc, rout, rerr.replace(ref, exe)) == (rc, out, err)
+
+
+def test_rw_experiment_saba_reports_an_unreadable_graph(runners, tmp_path):
+    # the reference lets this exception escape (the process aborts); here it is a message and exit 1
+    rc, out, err = _run(os.path.join(runners, "rw_experiment_saba"), ["nofolder", "ds", "5", "16"],
+                        tmp_path)
+    assert (rc, out, err) == (1, "", "rw_experiment_saba: cannot open graph: nofolder/ds/graph.txt")
