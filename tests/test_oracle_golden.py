@@ -100,3 +100,48 @@ def test_sampled_exact_matches_dense_exact():
     slots = np.random.default_rng(0).choice(len(adj), 200, replace=False)
     got = exact_sc.sampled_scores(idx, adj, slots)
     assert np.max(np.abs(got - exact[slots])) < 1e-9
+
+
+def _csr(n, edges):
+    rows = [[] for _ in range(n)]
+    for u, v in edges:
+        rows[u].append(v)
+        rows[v].append(u)
+    idx = np.zeros(n + 1, np.uint32)
+    idx[1:] = np.cumsum([len(r) for r in rows])
+    adj = np.array([x for r in rows for x in sorted(r)], np.uint32)
+    return idx, adj
+
+
+def test_exact_oracle_known_answers():
+    """Closed forms of the effective resistance of an edge: (n-1)/n on the cycle C_n, 2/n on K_n,
+    1 on every edge of a tree; Foster's theorem (the resistances of all edges sum to n - 1) on a
+    random graph; the sampled-edge oracle gives the same values."""
+    from oracle import exact_sc
+    from tgtp_b200 import synth
+
+    n = 9
+    idx, adj = _csr(n, [(k, (k + 1) % n) for k in range(n)])
+    assert np.allclose(exact_sc.exact_scores(idx, adj), (n - 1) / n, rtol=0, atol=1e-12)
+    assert np.allclose(exact_sc.sampled_scores(idx, adj, np.arange(len(adj))), (n - 1) / n,
+                       rtol=0, atol=1e-9)
+    n = 12
+    idx, adj = _csr(n, [(x, y) for x in range(n) for y in range(x + 1, n)])
+    assert np.allclose(exact_sc.exact_scores(idx, adj), 2 / n, rtol=0, atol=1e-12)
+    rng = np.random.default_rng(1)
+    n = 50
+    idx, adj = _csr(n, [(k, int(rng.integers(0, k))) for k in range(1, n)])
+    assert np.allclose(exact_sc.exact_scores(idx, adj), 1.0, rtol=0, atol=1e-12)
+    g = synth.chung_lu(300, 1500, 2.3, 5)
+    idx, adj = g.csr()
+    exact = exact_sc.exact_scores(idx, adj)
+    assert abs(exact.sum() / 2 - (g.n - 1)) < 1e-9 * g.n
+
+
+def test_reference_scores_on_complete_graph_are_within_eps_of_2_over_n(manifest):
+    """The reference's own scores on K_12 against the closed form 2/n, at every golden epsilon."""
+    c = golden_tgtp_case(manifest, "complete12")
+    n = len(c["idx"]) - 1
+    for run in c["runs"]:
+        s = load_golden_scores(run).astype(np.float64)
+        assert np.max(np.abs(s - 2 / n)) <= run["epsilon"], run
