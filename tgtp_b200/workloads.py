@@ -1,11 +1,16 @@
 """Seeded workloads from the command line, for profiling and quick checks on a GPU.
 
     python -m tgtp_b200.workloads aesc --graph config1 --eps 0.005 --precision mixed [--repeat 2]
+    python -m tgtp_b200.workloads aesc --graph config4 --eps 0.005 --precision mixed \
+        --vectors bf16 --deadline 600
     python -m tgtp_b200.workloads saba --graph config3 --depth 5 --walks 2048 [--repeat 2]
 
 Graphs: config1 (Chung-Lu n=4,039, 88,234 edges, exponent 2.5), config3 (R-MAT scale 18, edge
-factor 16, a=0.57), sparse5k (Chung-Lu n=5,000, 12,000 edges, exponent 2.1).  AESC inputs get
-128 eigenpairs from the scipy eigen prep.  Prints one line per run: seconds and work counters.
+factor 16, a=0.57), config4 (Chung-Lu n=10^6, 10^7 edges, exponent 2.3, seed 4), sparse5k
+(Chung-Lu n=5,000, 12,000 edges, exponent 2.1).  AESC inputs get 128 eigenpairs: from the scipy
+eigen prep (written and parsed back as sorted_eigens_128.txt) up to 20,000 vertices, from the GPU
+eigen prep (tolerance 1e-4) above.  --deadline sets the device time budget of one kernel
+(TGTP_KERNEL_DEADLINE_S; default 30 s).  Prints one line per run: seconds and work counters.
 """
 from __future__ import annotations
 
@@ -24,7 +29,29 @@ def _graph(name: str):
         return synth.config3_graph(1)
     if name == "sparse5k":
         return synth.chung_lu(5000, 12000, 2.1, 7)
+    if name == "config4":
+        return synth.chung_lu(1_000_000, 10_000_000, 2.3, 4)
     raise SystemExit(f"unknown graph {name}")
+
+
+def _eigenpairs(g, omega: int):
+    """(values, F32 vectors, F64 vectors), vertex-major as the loaders return them."""
+    import numpy as np
+
+    from . import aesc as A
+
+    if g.n <= 20_000:
+        from . import eigenprep, synth
+
+        d = tempfile.mkdtemp(prefix="tgtp_workload_")
+        synth.write_graph_txt(g, os.path.join(d, "graph.txt"))
+        return A.load_eigens_txt(eigenprep.eigenprep_folder(d, omega), g.n, omega)
+    from . import eigenprep_gpu
+
+    values, vecs, _, _, _ = eigenprep_gpu.compute(g.n, g.u, g.v, omega, seed=1, tol=1e-4,
+                                                  max_iter=60)
+    v64 = np.ascontiguousarray(vecs.T).ravel()
+    return values, v64.astype(np.float32), v64
 
 
 def main(argv=None) -> int:
@@ -37,7 +64,11 @@ def main(argv=None) -> int:
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--walks", type=int, default=2048)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--deadline", type=float, default=None,
+                    help="device time budget of one kernel, seconds (TGTP_KERNEL_DEADLINE_S)")
     args = ap.parse_args(argv)
+    if args.deadline is not None:
+        os.environ["TGTP_KERNEL_DEADLINE_S"] = repr(args.deadline)
 
     from . import aesc as A
 
@@ -52,15 +83,7 @@ def main(argv=None) -> int:
                   f"visit_count {vc} checksum {cs} fallback_bouquets {fb}", flush=True)
         dg.free()
         return 0
-    from . import eigenprep
-
-    d = tempfile.mkdtemp(prefix="tgtp_workload_")
-    synth_path = os.path.join(d, "graph.txt")
-    from . import synth
-
-    synth.write_graph_txt(g, synth_path)
-    path = eigenprep.eigenprep_folder(d, 128)
-    values, v32, v64 = A.load_eigens_txt(path, g.n, 128)
+    values, v32, v64 = _eigenpairs(g, 128)
     prec = {"fp32": A.PRECISION_FP32, "fp64": A.PRECISION_FP64, "mixed": A.PRECISION_MIXED}
     if args.precision == "fp64":
         dg.upload_eigens(values, v64, A.VEC_F64)
