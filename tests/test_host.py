@@ -135,6 +135,30 @@ def test_eigenprep_pairs_are_eigenpairs_of_the_random_walk_matrix(tmp_path):
     assert (tmp_path / "stat.txt").read_text().startswith("n=200\nm=")
 
 
+def test_gpu_eigen_prep_solver_matches_the_scipy_restatement_on_cpu():
+    """The Chebyshev-filtered subspace iteration of eigenprep_gpu, run with torch on the CPU: the
+    same eigenvalues as the scipy (Lanczos) restatement, sorted by |lambda| descending, each vector
+    an eigenvector of D^-1 A with sum_i deg_i x_i^2 = 2m, equal to scipy's up to sign (the
+    eigenvalues of this graph are separated by at least 2.9e-3)."""
+    from tgtp_b200 import eigenprep, eigenprep_gpu, synth
+
+    g = synth.chung_lu(600, 3000, 2.3, 9)
+    v1, x1, _ = eigenprep.compute(g.n, g.u, g.v, 16, seed=0)
+    v2, x2, m, _, worst = eigenprep_gpu.compute(g.n, g.u, g.v, 16, seed=1, tol=1e-10,
+                                                device="cpu")
+    assert worst < 1e-10
+    assert np.max(np.abs(v1 - v2)) < 1e-10
+    assert np.all(np.diff(np.abs(v2)) <= 1e-12)
+    idx, adj = g.csr()
+    deg = np.diff(idx.astype(np.int64)).astype(np.float64)
+    for lam, x, y in zip(v2, x2, x1):
+        ax = np.add.reduceat(x[adj], idx[:-1]) / deg
+        assert np.max(np.abs(ax - lam * x)) < 1e-8 * np.max(np.abs(x))
+        assert abs(np.dot(deg, x * x) - 2 * m) < 1e-8 * m
+        cos = np.dot(deg, x * y) / np.sqrt(np.dot(deg, x * x) * np.dot(deg, y * y))
+        assert abs(abs(cos) - 1) < 1e-8
+
+
 def test_input_cache_reuses_parsed_inputs_and_follows_the_text(tmp_path, monkeypatch, manifest, tgtp_lib):
     """TGTP_INPUT_CACHE=1: the loaders write '<file>.tgtpcache' beside the text, later loads read
     it and give the same arrays, and a change of the text file invalidates it."""
