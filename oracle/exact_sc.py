@@ -1,10 +1,14 @@
 """TEST INFRASTRUCTURE ONLY: exact edge spanning centrality (effective resistance) per CSR slot.
 
-Restates scripts/paper_accuracy.py:13-54 (and src/exact_sc.cpp:15-55): per connected component, the
-grounded Laplacian (last vertex removed) is factored by dense Cholesky and inverted; the score of
-slot (u, v) is G[u,u] + G[v,v] - 2 G[u,v] with G the inverse padded by a zero row / column.  The
-solve is certified on seeded probe vectors and by Foster's theorem (the undirected scores sum to
-n - #components), as the reference script does.  Dense, so for graphs up to ~20k vertices.
+The quantity of scripts/paper_accuracy.py:13-54 and src/exact_sc.cpp:15-55: for the slot (u, v),
+R(u, v) = (e_u - e_v)^T L^+ (e_u - e_v) on the simple undirected graph of the CSR (repeated slots
+count once, self-loops are ignored; a self-loop slot scores 0).  Computed per connected component C
+of k vertices from M = (L_C + J/k)^-1, J the all-ones matrix: L_C + J/k is symmetric positive
+definite (J/k lifts the one zero eigenvalue of L_C, on the constant vector, to 1), its inverse is
+L_C^+ + J/k, and the J/k part cancels in R, so R(u, v) = M[u,u] + M[v,v] - 2 M[u,v] from one dense
+Cholesky factorisation per component.  Certified by the factorisation's residual on seeded probe
+columns and by Foster's theorem (the undirected resistances sum to n - #components).  Dense, so
+for graphs up to ~20k vertices; `sampled_scores` covers larger ones.
 """
 from __future__ import annotations
 
@@ -17,35 +21,37 @@ def exact_scores(idx: np.ndarray, adj: np.ndarray) -> np.ndarray:
     from scipy.sparse.csgraph import connected_components
 
     n = len(idx) - 1
-    m = int(idx[-1])
-    rows = np.repeat(np.arange(n), np.diff(idx.astype(np.int64)))
-    cols = adj.astype(np.int64)
-    a = csr_matrix((np.ones(m), (rows, cols)), shape=(n, n))
-    ncomp, labels = connected_components(a, directed=False)
-    result = np.zeros(m)
-    worst = 0.0
-    for comp in range(ncomp):
-        nodes = np.flatnonzero(labels == comp)
-        sub = a[nodes][:, nodes].toarray()
-        lap = np.diag(sub.sum(axis=1)) - sub
-        grounded = lap[:-1, :-1]
-        if grounded.size == 0:
-            continue
-        factor = cho_factor(grounded, lower=True)
-        inverse = cho_solve(factor, np.eye(len(nodes) - 1))
-        probe = np.random.default_rng(42).normal(size=(len(nodes) - 1, 4))
-        worst = max(worst, float(np.max(np.abs(grounded @ cho_solve(factor, probe) - probe))))
-        green = np.zeros((len(nodes), len(nodes)))
-        green[:-1, :-1] = inverse
-        local = np.full(n, -1, dtype=np.int64)
-        local[nodes] = np.arange(len(nodes))
-        pos = np.flatnonzero(labels[rows] == comp)
-        u, v = local[rows[pos]], local[cols[pos]]
-        result[pos] = green[u, u] + green[v, v] - 2 * green[u, v]
-    foster = abs(result.sum() / 2 - (n - ncomp))
-    if not np.all(np.isfinite(result)) or worst > 1e-6 or foster > 1e-5 * max(1, n):
-        raise RuntimeError("exact reference failed residual/Foster checks")
-    return result
+    src = np.repeat(np.arange(n), np.diff(idx.astype(np.int64)))
+    dst = adj.astype(np.int64)
+    off = src != dst
+    simple = csr_matrix((np.ones(int(off.sum())), (src[off], dst[off])), shape=(n, n))
+    simple.sum_duplicates()
+    simple.data[:] = 1.0  # one edge per vertex pair
+    ncomp, comp_of = connected_components(simple, directed=False)
+    out = np.zeros(len(dst))
+    residual = 0.0
+    undirected_sum = 0.0
+    probes = np.random.default_rng(7)
+    for c in range(ncomp):
+        members = np.flatnonzero(comp_of == c)  # ascending: local index by searchsorted
+        k = len(members)
+        block = simple[members][:, members].toarray()
+        shifted = np.diag(block.sum(axis=1)) - block + 1.0 / k
+        factor = cho_factor(shifted, lower=True)
+        inv = cho_solve(factor, np.eye(k))
+        z = probes.standard_normal((k, 4))
+        residual = max(residual, float(np.max(np.abs(shifted @ (inv @ z) - z))))
+        slots = np.flatnonzero(off & (comp_of[src] == c))
+        lu = np.searchsorted(members, src[slots])
+        lv = np.searchsorted(members, dst[slots])
+        out[slots] = inv[lu, lu] + inv[lv, lv] - 2.0 * inv[lu, lv]
+        iu, iv = np.nonzero(np.triu(block, 1))
+        undirected_sum += float(np.sum(inv[iu, iu] + inv[iv, iv] - 2.0 * inv[iu, iv]))
+    foster = abs(undirected_sum - (n - ncomp))
+    if not np.all(np.isfinite(out)) or residual > 1e-6 or foster > 1e-5 * max(1, n):
+        raise RuntimeError(f"exact spanning centrality not certified: probe residual {residual:.3g}, "
+                           f"Foster deviation {foster:.3g}")
+    return out
 
 
 def accuracy(scores: np.ndarray, exact: np.ndarray, eps: float) -> dict:
