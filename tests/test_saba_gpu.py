@@ -109,10 +109,13 @@ def test_saba_rmat18_counters_match_oracle_at_full_graph_size(cuda_device, oracl
     dg.free()
 
 
-def test_saba_rmat18_benchmark_size_two_kernels_agree(cuda_device):
-    """The benchmark configuration (depth 5, 2,048 walks per vertex, 1.78e9 transitions): the
-    degree-renumbered kernel of saba_count and the plain kernel behind saba_count_static give the
-    same visit count, checksum and fallback count, and visit_count = n * W * D exactly."""
+@pytest.mark.parametrize("depth,walks", [(5, 2048), (15, 16384)])
+def test_saba_rmat18_benchmark_size_two_kernels_agree(cuda_device, depth, walks):
+    """The benchmark configuration (depth 5, 2,048 walks per vertex, 1.78e9 transitions) and the
+    largest one (depth 15, 16,384 walks, 4.3e10 transitions; its largest counter is about 1.6e8,
+    1,024 times the oracle's 155,643 at 16 walks, far below 2^32): the degree-renumbered kernel of saba_count and the plain kernel behind
+    saba_count_static give the same visit count, checksum and fallback count, and
+    visit_count = n * W * D exactly."""
     import ctypes as C
 
     import torch
@@ -123,14 +126,14 @@ def test_saba_rmat18_benchmark_size_two_kernels_agree(cuda_device):
     g = synth.config3_graph(1)
     idx, adj = g.csr()
     dg = AESCGraph.from_csr(idx, adj)
-    _, visits, checksum, fallbacks = saba_count(dg, 5, 2048, counters=False)
-    assert visits == g.n * 2048 * 5
+    _, visits, checksum, fallbacks = saba_count(dg, depth, walks, counters=False)
+    assert visits == g.n * walks * depth
     d_idx = torch.from_numpy(idx.astype(np.int32)).cuda()
     d_adj = torch.from_numpy(adj.astype(np.int32)).cuda()
     torch.cuda.synchronize()
     res = _lib.SabaResult()
     _lib.check(_lib.lib().saba_count_static(C.c_void_p(d_idx.data_ptr()),
-                                            C.c_void_p(d_adj.data_ptr()), g.n, 5, 2048, None,
+                                            C.c_void_p(d_adj.data_ptr()), g.n, depth, walks, None,
                                             C.byref(res)))
     assert (int(res.visit_count), int(res.checksum), int(res.fallback_bouquets)) == (
         visits, checksum, fallbacks)
