@@ -77,6 +77,70 @@ def test_eigen_loader_rejects_short_and_nonfinite(tmp_path, tgtp_lib):
         load_eigens_txt(str(p), 2, 2)
 
 
+def _eigen_text(n, omega, seed):
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(omega):
+        x = rng.standard_normal(n) * 10.0 ** rng.integers(-30, 3, n)
+        rows.append(" ".join(["%.17g" % (1 - i / omega)] + ["%.17g" % v for v in x.tolist()]))
+    return rows
+
+
+def test_eigen_loader_parallel_chunks_agree_with_sequential_reading(tmp_path, tgtp_lib, oracle_lib):
+    """A 19 MB eigen file is read in many chunks on several threads: the same bits as the oracle's
+    sequential parser, the first bad number in file order decides the error (eigenvalue or
+    eigenvector), a file that ends early is rejected, and text after the numbers that are needed
+    is never examined."""
+    from tgtp_b200.aesc import TgtpError, load_eigens_txt
+
+    n, omega = 50000, 16
+    rows = _eigen_text(n, omega, 5)
+    path = tmp_path / "sorted_eigens_16.txt"
+    path.write_text("\n".join(rows) + "\n")
+    assert path.stat().st_size > 16 << 20
+    got = load_eigens_txt(str(path), n, omega)
+    want = oracle_lib.parse_eigens(str(path), n, omega)
+    for x, y in zip(got, want):
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+    # glued numbers ("a-b") are two numbers, read the same way
+    glued = list(rows)
+    toks = glued[7].split(" ")
+    glued[7] = " ".join(toks[:100] + [toks[100] + "-0.25"] + toks[102:])
+    path.write_text("\n".join(glued) + "\n")
+    got = load_eigens_txt(str(path), n, omega)
+    want = oracle_lib.parse_eigens(str(path), n, omega)
+    for x, y in zip(got, want):
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+
+    def rejected(text, message):
+        path.write_text(text)
+        with pytest.raises(TgtpError) as e:
+            load_eigens_txt(str(path), n, omega)
+        assert e.value.message == f"{message} in {path}"
+
+    def with_token(rs, r, j, tok):
+        rs = list(rs)
+        t = rs[r].split(" ")
+        t[j] = tok
+        rs[r] = " ".join(t)
+        return rs
+
+    rejected("\n".join(with_token(rows, 14, 40000, "abc")) + "\n", "invalid eigenvector")
+    rejected("\n".join(with_token(rows, 3, 17, "1e999")) + "\n", "invalid eigenvector")
+    both = with_token(with_token(rows, 12, 0, "x"), 14, 5, "y")
+    rejected("\n".join(both) + "\n", "invalid eigenvalue")
+    early = with_token(with_token(rows, 14, 5, "y"), 12, 30000, "x")
+    rejected("\n".join(early) + "\n", "invalid eigenvector")
+    rejected("\n".join(rows[:10]) + "\n", "invalid eigenvalue")
+    rejected("\n".join(rows[:15]) + "\n" + " ".join(rows[15].split(" ")[:20000]),
+             "invalid eigenvector")
+    path.write_text("\n".join(rows) + "\nnot numbers after the last pair 1e999 nan\n")
+    got = load_eigens_txt(str(path), n, omega)
+    want = oracle_lib.parse_eigens(str(path), n, omega)
+    for x, y in zip(got, want):
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+
+
 def test_eigen_loader_agrees_with_oracle_parser_on_golden_files(manifest, tgtp_lib, oracle_lib):
     from tgtp_b200.aesc import load_eigens_txt
 

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -156,6 +157,118 @@ void cache_write(const char* path, const char* magic, uint64_t a, uint64_t b,
     ok = std::fclose(f) == 0 && ok;
     if (!ok || std::rename(tmp.c_str(), dst.c_str()) != 0) std::remove(tmp.c_str());
 }
+
+// ---- parallel reader of decimal numbers ----------------------------------------------------------
+// The eigen file of a 10^6-vertex graph holds ~1.3e8 numbers; read one after another they take
+// tens of seconds.  read_numbers gives the result of the sequential reader (skip whitespace, take
+// the longest decimal prefix, repeat; stop at the first spot that starts no number) on several
+// threads: the text is cut into chunks at whitespace, so no number spans two chunks; a first pass
+// counts the numbers of each chunk up to its first unreadable spot, a second pass converts each
+// chunk's numbers with their global index k.  Numbers past the `need` first are not examined, as
+// the sequential reader never reaches them.
+struct NumberChunk {
+    const char* begin;
+    const char* end;
+    uint64_t count = 0;    // numbers before the chunk's first unreadable spot (or its end)
+    bool stopped = false;  // an unreadable spot was met
+    uint64_t first = 0;    // global index of the chunk's first number
+};
+
+unsigned reader_threads(size_t bytes) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t by_size = bytes / (size_t(4) << 20) + 1;  // at least 4 MB of text per thread
+    return unsigned(std::min<size_t>({size_t(hw), size_t(32), by_size}));
+}
+
+template <class F>
+void parallel_for(size_t count, unsigned threads, F&& body) {
+    if (threads <= 1 || count <= 1) {
+        for (size_t i = 0; i < count; ++i) body(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const unsigned t = unsigned(std::min<size_t>(threads, count));
+    pool.reserve(t);
+    for (unsigned w = 0; w < t; ++w) {
+        auto share = [&, w] {
+            for (size_t i = w; i < count; i += t) body(i);
+        };
+        if (w + 1 == t) {  // the calling thread takes the last share
+            share();
+            break;
+        }
+        try {
+            pool.emplace_back(share);
+        } catch (...) {  // no thread to be had: this share runs here
+            share();
+        }
+    }
+    for (auto& th : pool) th.join();
+}
+
+// convert(k, token, len) converts number k (a NUL-terminated copy of its text) and returns false
+// when the value is not acceptable.  Returns the index of the first number the sequential reader
+// rejects or cannot find (the file's end included), or `need` when the first `need` numbers are
+// all read and accepted.
+template <class Convert>
+uint64_t read_numbers(const char* data, size_t size, uint64_t need, Convert&& convert) {
+    const char* end = data + size;
+    const unsigned threads = reader_threads(size);
+    std::vector<NumberChunk> chunks;
+    const size_t target = std::max<size_t>(size / (size_t(threads) * 4) + 1, size_t(1) << 20);
+    for (const char* b = data; b < end;) {
+        const char* e = b + std::min(target, size_t(end - b));
+        while (e < end && !is_ws(*e)) ++e;  // cut at whitespace
+        chunks.push_back(NumberChunk{b, e});
+        b = e;
+    }
+    parallel_for(chunks.size(), threads, [&](size_t c) {
+        NumberChunk& ch = chunks[c];
+        for (const char* p = ch.begin;;) {
+            while (p < ch.end && is_ws(*p)) ++p;
+            if (p >= ch.end) break;
+            const size_t len = float_prefix(p, ch.end);
+            if (!len) {
+                ch.stopped = true;
+                break;
+            }
+            ++ch.count;
+            p += len;
+        }
+    });
+    // limit: the index where the sequential reader stops (first unreadable spot, end of file or
+    // `need`); chunks behind an unreadable spot start at or past it and are not converted
+    uint64_t upto = 0, limit = UINT64_MAX;
+    for (NumberChunk& ch : chunks) {
+        ch.first = upto;
+        upto += ch.count;
+        if (ch.stopped && limit == UINT64_MAX) limit = upto;
+    }
+    limit = std::min({limit, upto, need});
+    std::vector<uint64_t> bad(chunks.size(), UINT64_MAX);
+    parallel_for(chunks.size(), threads, [&](size_t c) {
+        const NumberChunk& ch = chunks[c];
+        if (ch.first >= limit) return;
+        std::string tok;
+        uint64_t k = ch.first;
+        for (const char* p = ch.begin; k < limit;) {
+            while (p < ch.end && is_ws(*p)) ++p;
+            if (p >= ch.end) break;
+            const size_t len = float_prefix(p, ch.end);
+            if (!len) break;
+            tok.assign(p, len);
+            p += len;
+            if (!convert(k, tok.c_str())) {
+                bad[c] = k;
+                return;
+            }
+            ++k;
+        }
+    });
+    uint64_t first_bad = limit;
+    for (uint64_t b : bad) first_bad = std::min(first_bad, b);
+    return first_bad;
+}
 }  // namespace
 }  // namespace tgtp
 
@@ -290,31 +403,32 @@ tgtp_status tgtp_load_eigens_txt(const char* path, uint64_t n, uint32_t omega, d
                 out64 = keep64.data();
             }
         }
-        const char* p = f.data;
-        const char* end = f.data + f.size;
-        std::string tok;
-        auto next = [&](double* d, float* fl) -> bool {
-            while (p < end && is_ws(*p)) ++p;
-            const size_t len = float_prefix(p, end);
-            if (!len) return false;
-            tok.assign(p, len);
-            p += len;
-            if (d) *d = std::strtod(tok.c_str(), nullptr);
-            if (fl) *fl = std::strtof(tok.c_str(), nullptr);
-            return (!d || std::isfinite(*d)) && (!fl || std::isfinite(*fl));
-        };
-        for (uint32_t i = 0; i < omega; ++i) {
-            if (!next(&values[i], nullptr))
-                fail(TGTP_ERR_IO, std::string("invalid eigenvalue in ") + path);
-            for (uint64_t j = 0; j < n; ++j) {
-                double d;
-                float fl;
-                if (!next(out64 ? &d : nullptr, out32 ? &fl : (out64 ? nullptr : &fl)))
-                    fail(TGTP_ERR_IO, std::string("invalid eigenvector in ") + path);
-                if (out32) out32[j * omega + i] = fl;
-                if (out64) out64[j * omega + i] = d;
+        // number k of the file: k = i (n + 1) is eigenvalue i, the n after it its vector; the
+        // vector entries are stored vertex-major (entry j of pair i at j * omega + i)
+        const uint64_t row = n + 1;
+        const uint64_t need = uint64_t(omega) * row;
+        const uint64_t stop = read_numbers(f.data, f.size, need, [&](uint64_t k, const char* tok) {
+            const uint64_t i = k / row, j = k % row;
+            if (j == 0) {
+                values[i] = std::strtod(tok, nullptr);
+                return bool(std::isfinite(values[i]));
             }
-        }
+            const size_t at = size_t(j - 1) * omega + i;
+            bool ok = true;
+            if (out64) {
+                out64[at] = std::strtod(tok, nullptr);
+                ok = std::isfinite(out64[at]);
+            }
+            if (out32 || !out64) {
+                const float fl = std::strtof(tok, nullptr);
+                if (out32) out32[at] = fl;
+                ok = ok && std::isfinite(fl);
+            }
+            return ok;
+        });
+        if (stop < need)
+            fail(TGTP_ERR_IO, std::string(stop % row == 0 ? "invalid eigenvalue in "
+                                                           : "invalid eigenvector in ") + path);
         if (cache_enabled())
             cache_write(path, "TGTPEIG1", n, omega,
                         {{values, sizeof(double) * omega},
