@@ -252,3 +252,13 @@ def test_input_cache_reuses_parsed_inputs_and_follows_the_text(tmp_path, monkeyp
         f.write(f"0 {c['n'] - 1}\n")
     g2 = load_graph_txt(str(gpath))
     assert int(g2[0][-1]) == int(plain_g[0][-1]) + 2  # the loader mirrors and keeps every line
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library there is no fallback: the first call raises."""
+    from tgtp_b200 import _lib
+
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libtgtp_gpu.so"))
+    with pytest.raises(RuntimeError, match="is missing"):
+        _lib.lib()
