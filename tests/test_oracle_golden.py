@@ -145,3 +145,49 @@ def test_reference_scores_on_complete_graph_are_within_eps_of_2_over_n(manifest)
     for run in c["runs"]:
         s = load_golden_scores(run).astype(np.float64)
         assert np.max(np.abs(s - 2 / n)) <= run["epsilon"], run
+
+
+@pytest.fixture(scope="module")
+def omega128_case(tmp_path_factory):
+    """A Chung-Lu graph (1,200 vertices, 9,000 edges) with 128 eigenpairs in the reference's file
+    layout, for the reference binary and the oracle."""
+    from tgtp_b200 import eigenprep, synth
+    from tgtp_b200.aesc import load_eigens_txt
+
+    root = tmp_path_factory.mktemp("omega128")
+    g = synth.chung_lu(1200, 9000, 2.4, 21)
+    (root / "g").mkdir()
+    synth.write_graph_txt(g, str(root / "g" / "graph.txt"))
+    path = eigenprep.eigenprep_folder(str(root / "g"), 128)
+    idx, adj = g.csr()
+    values, v32, v64 = load_eigens_txt(path, g.n, 128)
+    return dict(root=root, idx=idx, adj=adj, values=values, v32=v32, v64=v64)
+
+
+@pytest.mark.parametrize("eps", [0.05, 0.01, 0.005])
+def test_oracle_matches_the_reference_binary_at_omega_128(omega128_case, oracle_lib, tgtp_lib,
+                                                          eps):
+    """The golden fixtures use omega <= 16; at the path's omega = 128 the reference's own tgtp
+    (oracle/_ref/tgtp_O2, run here) pins the oracle: FP32 bit-exact, FP64 within 1e-6 relative
+    (or 2 float32 ulps) on every slot."""
+    import subprocess
+
+    from conftest import ROOT
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "tgtp_O2")
+    if not os.path.exists(exe):
+        pytest.skip("the reference binaries are not built (oracle/_ref)")
+    c = omega128_case
+    out = c["root"] / f"scores_{eps}.bin"
+    r = subprocess.run([exe, str(c["root"]), "g", str(eps), "128", "10", str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    want = np.fromfile(out, dtype=np.float32)
+    got, det = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v32"], eps, gamma=10,
+                               details=True)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    if eps == 0.005:
+        assert det["stats"]["walk_hops"] > 0  # the walk phase is part of what is pinned
+    got64 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], eps, gamma=10, fp64=True)
+    tol = np.maximum(1e-6 * np.abs(want), 2 * np.spacing(np.abs(want)))
+    assert np.all(np.abs(got64.astype(np.float64) - want) <= tol)
