@@ -191,3 +191,32 @@ def test_oracle_matches_the_reference_binary_at_omega_128(omega128_case, oracle_
     got64 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], eps, gamma=10, fp64=True)
     tol = np.maximum(1e-6 * np.abs(want), 2 * np.spacing(np.abs(want)))
     assert np.all(np.abs(got64.astype(np.float64) - want) <= tol)
+
+
+@pytest.mark.parametrize("graph,depth,walks", [("config1", 5, 2048), ("rmat14", 10, 64)])
+def test_saba_oracle_matches_the_reference_walks_at_benchmark_size(tmp_path, oracle_lib, tgtp_lib,
+                                                                  graph, depth, walks):
+    """The SABA walk configuration of the benchmark (the 4,039-vertex graph, depth 5, 2,048 walks)
+    and an R-MAT scale-14 graph: every counter of the oracle equal to the reference's own walk
+    routine (oracle/_ref/saba_harness_O2, run here; its float counters stay below 2^24 here)."""
+    import subprocess
+
+    from conftest import ROOT
+    from tgtp_b200 import synth
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "saba_harness_O2")
+    if not os.path.exists(exe):
+        pytest.skip("the reference binaries are not built (oracle/_ref)")
+    g = synth.config1_graph(1) if graph == "config1" else synth.rmat(14, 8, 0.57, 0.19, 0.19, 3)
+    synth.write_graph_txt(g, str(tmp_path / "graph.txt"))
+    out = tmp_path / "counts.u32"
+    r = subprocess.run([exe, str(tmp_path / "graph.txt"), str(depth), str(walks), str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    want = np.fromfile(out, dtype=np.uint32).astype(np.uint64)
+    idx, adj = g.csr()
+    got = oracle_lib.saba(idx, adj, depth, walks)
+    assert np.array_equal(got, want)
+    n, m, visits, checksum = (int(x) for x in r.stdout.split())
+    assert (n, m) == (g.n, len(adj)) and visits == int(got.sum())
+    assert checksum == int((got * np.arange(1, n + 1, dtype=np.uint64)).sum())
