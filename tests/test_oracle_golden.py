@@ -220,3 +220,16 @@ def test_saba_oracle_matches_the_reference_walks_at_benchmark_size(tmp_path, ora
     n, m, visits, checksum = (int(x) for x in r.stdout.split())
     assert (n, m) == (g.n, len(adj)) and visits == int(got.sum())
     assert checksum == int((got * np.arange(1, n + 1, dtype=np.uint64)).sum())
+
+
+@pytest.mark.parametrize("name", TGTP_CASES)
+def test_exact_oracle_matches_the_reference_accuracy_script(manifest, name):
+    """oracle/exact_sc.py against the exact scores of the reference's scripts/paper_accuracy.py
+    (tests/golden/exact/, made by tests/golden/make_exact.py) on the golden graphs."""
+    from oracle import exact_sc
+
+    c = golden_tgtp_case(manifest, name)
+    want = np.load(os.path.join(GOLDEN, "exact", f"{name}.npy"))
+    got = exact_sc.exact_scores(c["idx"], c["adj"])
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) < 1e-12
