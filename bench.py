@@ -118,6 +118,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (first processor of /proc/cpuinfo), or the platform's answer."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def cpu_baseline_line(edges: int, secs_all, threads: int, secs_one, sample: str) -> dict:
+    """cpu_baseline of the JSON line: the reference on all host cores (the value), the same on one
+    core beside it, the core count, OMP_NUM_THREADS and the CPU model."""
+    out = {"value": edges / min(secs_all), "unit": "edges/s", "cores": threads,
+           "kind": "reference", "omp_num_threads": threads, "cpu_model": cpu_model(),
+           "sample": sample}
+    if secs_one:
+        out["single_thread"] = {"value": edges / min(secs_one), "unit": "edges/s", "cores": 1,
+                                "sample": "min of 3 tgtp() calls (after 1 warm-up), "
+                                          "OMP_NUM_THREADS=1"}
+    return out
+
+
 def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int, warmups: int):
     """The reference's own benchmark binary (compiled from its sources into oracle/_ref)."""
     import oracle
@@ -320,6 +347,7 @@ def run_reference_arm(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Chung-Lu + scipy eigenpairs)",
         "config": {"workload": WORKLOAD, "graph_seed": 1, "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "reference",
+                         "omp_num_threads": threads, "cpu_model": cpu_model(),
                          "sample": f"{args.steps} timed tgtp() calls after {args.warmup} warm-up, "
                                    "reference benchmark binary (-Ofast -march=x86-64-v3, OpenMP)"},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
@@ -514,10 +542,10 @@ def main():
             threads = os.cpu_count() or 1
             secs = cpu_reference_run(root, "cl4039", threads, 5, 1)
             if secs:
-                cpu = {"value": E / min(secs), "unit": "edges/s", "cores": threads,
-                       "kind": "reference",
-                       "sample": "min of 5 tgtp() calls (after 1 warm-up) of the reference "
-                                 "benchmark binary on the same graph and eigen files"}
+                one = cpu_reference_run(root, "cl4039", 1, 3, 1)
+                cpu = cpu_baseline_line(E, secs, threads, one,
+                                        "min of 5 tgtp() calls (after 1 warm-up) of the reference "
+                                        "benchmark binary on the same graph and eigen files")
         line = {
             "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,

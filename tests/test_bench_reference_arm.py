@@ -36,6 +36,7 @@ def test_reference_arm_prints_the_contract_line():
     assert abs(d["ms_per_step"] * 1e-3 * d["value"] - 88234) < 1e-6 * 88234
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1
+    assert cb["omp_num_threads"] == cb["cores"] and cb["cpu_model"]
     assert d["e2e"] == {"value": d["value"], "unit": "edges/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]
@@ -43,3 +44,16 @@ def test_reference_arm_prints_the_contract_line():
 
 def test_reference_arm_runs_on_rank_zero_only():
     assert _bench("--steps", "1", "--warmup", "3", env={"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def test_cpu_baseline_line_reports_both_thread_counts():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    line = bench.cpu_baseline_line(1000, [0.5, 0.25], 16, [2.0, 4.0], "sample")
+    assert line["value"] == 4000 and line["cores"] == 16 and line["omp_num_threads"] == 16
+    assert line["single_thread"]["value"] == 500 and line["single_thread"]["cores"] == 1
+    assert line["cpu_model"] and line["kind"] == "reference"
+    assert "single_thread" not in bench.cpu_baseline_line(1000, [0.5], 16, None, "sample")
