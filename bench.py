@@ -162,6 +162,38 @@ def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int
     return secs
 
 
+def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3):
+    """The reference's rw_experiment_saba (built from its sources into oracle/_ref) on `g`, on all
+    host cores: the fastest of `runs` runs, as transitions per second of its own walk timer, or None
+    when the binary is missing or fails."""
+    import oracle
+    from tgtp_b200 import synth
+
+    exe = oracle.ref_binary("rw_experiment_saba")
+    if exe is None:
+        return None
+    folder = os.path.join(root, "saba_data")
+    os.makedirs(os.path.join(folder, "g"), exist_ok=True)
+    synth.write_graph_txt(g, os.path.join(folder, "g", "graph.txt"))
+    threads = os.cpu_count() or 1
+    walk_s = []
+    for _ in range(runs):
+        r = subprocess.run([exe, folder, "g", str(depth), str(walks), str(threads)],
+                           capture_output=True, text=True, cwd=root, timeout=900,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        if r.returncode != 0:
+            return None
+        # TSV fields (src/rw_experiment_saba.cpp:241-244): 8 = t_rw_s, 10 = total_walks, which
+        # already counts every hop (n * n_walks * depth): transitions
+        f = r.stdout.strip().splitlines()[-1].split("\t")
+        walk_s.append((float(f[8]), float(f[10])))
+    t_rw, total = min(walk_s)
+    return {"transitions_per_s": total / t_rw, "transitions": total, "cores": threads,
+            "omp_num_threads": threads, "walk_seconds": t_rw,
+            "sample": f"min of {runs} runs of the reference rw_experiment_saba (-Ofast, OpenMP) "
+                      "on the same graph"}
+
+
 def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
     """SABA walk counter at scale: seeded R-MAT scale 18, edge factor 16 (a=0.57, b=c=0.19), largest
     component; depth 5, 2048 walks per vertex.  Kernel time from the library's CUDA events (3 runs
@@ -189,23 +221,9 @@ def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
            "hbm_frac_of_" + peak_kind: trans * 20 / (ms * 1e-3) / 1e9 / hbm,
            "visit_count": vc, "checksum": cs, "fallback_bouquets": fb}
     if with_cpu:
-        import oracle
-
-        exe = oracle.ref_binary("rw_experiment_saba")
-        if exe is not None:
-            folder = os.path.join(root, "saba_data")
-            os.makedirs(os.path.join(folder, "rmat18"), exist_ok=True)
-            synth.write_graph_txt(g, os.path.join(folder, "rmat18", "graph.txt"))
-            threads = os.cpu_count() or 1
-            r = subprocess.run([exe, folder, "rmat18", "5", "2048", str(threads)],
-                               capture_output=True, text=True, cwd=root, timeout=900,
-                               env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
-            if r.returncode == 0:
-                f = r.stdout.strip().splitlines()[-1].split("\t")
-                out["cpu_reference"] = {"transitions_per_s": float(f[11]) * 5, "cores": threads,
-                                        "walk_seconds": float(f[8]),
-                                        "sample": "one run of the reference rw_experiment_saba "
-                                                  "(-Ofast, OpenMP) on the same graph"}
+        ref = saba_cpu_reference(g, root, 5, 2048)
+        if ref is not None:
+            out["cpu_reference"] = ref
     return out
 
 

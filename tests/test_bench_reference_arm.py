@@ -57,3 +57,21 @@ def test_cpu_baseline_line_reports_both_thread_counts():
     assert line["single_thread"]["value"] == 500 and line["single_thread"]["cores"] == 1
     assert line["cpu_model"] and line["kind"] == "reference"
     assert "single_thread" not in bench.cpu_baseline_line(1000, [0.5], 16, None, "sample")
+
+
+def test_saba_cpu_reference_counts_transitions_once(tmp_path):
+    """The reference SABA runner's total_walks already counts every hop: the rate bench.py reports
+    is n * W * D over the runner's own walk time, the fastest of the runs."""
+    import importlib.util
+
+    from tgtp_b200 import synth
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    g = synth.rmat(12, 8, 0.57, 0.19, 0.19, 5)
+    ref = bench.saba_cpu_reference(g, str(tmp_path), 5, 64, runs=2)
+    if ref is None:  # the reference binaries under oracle/_ref were not built here
+        return
+    assert ref["transitions"] == g.n * 64 * 5
+    assert ref["transitions_per_s"] == ref["transitions"] / ref["walk_seconds"]
