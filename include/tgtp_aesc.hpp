@@ -40,6 +40,17 @@ inline int precision_from_env(int fallback = TGTP_PRECISION_FP32) {
     throw std::invalid_argument("TGTP_PRECISION must be fp32, fp64 or mixed");
 }
 
+// Device storage of the eigenvectors for the command-line runners: TGTP_VECTORS=f32 (default) |
+// bf16.  BF16 storage is read by the mixed form only, so it is refused with any other form.
+inline int vectors_from_env(int precision) {
+    const char* p = std::getenv("TGTP_VECTORS");
+    if (!p || !*p || std::string(p) == "f32") return TGTP_VEC_F32;
+    if (std::string(p) != "bf16") throw std::invalid_argument("TGTP_VECTORS must be f32 or bf16");
+    if (precision != TGTP_PRECISION_MIXED)
+        throw std::invalid_argument("TGTP_VECTORS=bf16 needs TGTP_PRECISION=mixed");
+    return TGTP_VEC_BF16;
+}
+
 // CSR as fuser::graph_t<uint32_t, uint32_t> builds it (src/graph.h:10-98), resident on the device.
 struct Graph {
     std::vector<uint32_t> idx, adj;  // host copies, same layout as graph_t::idx / graph_t::adj
@@ -74,8 +85,10 @@ struct Graph {
 // src/aesc.h:83-97: CSR + omega eigenpairs, validated as the reference does.
 struct AESCGraph : Graph {
     size_t omega = 0;
+    // vec_store: device storage of FP32/mixed-form vectors (TGTP_VEC_F32, or TGTP_VEC_BF16 for
+    // the mixed form); the FP64 form always stores FP64
     AESCGraph(const std::string& graph_path, const std::string& eigen_path, size_t omega_,
-              int precision = TGTP_PRECISION_FP32)
+              int precision = TGTP_PRECISION_FP32, int vec_store = TGTP_VEC_F32)
         : omega(omega_) {
         load_txt(graph_path);
         if (omega < 2 || omega > n) throw std::runtime_error("omega must be between 2 and vertex count");
@@ -93,7 +106,7 @@ struct AESCGraph : Graph {
                                      TGTP_VEC_F64, TGTP_VEC_F64));
         else
             check(tgtp_eigens_upload(handle, values.data(), v32.data(), uint32_t(omega),
-                                     TGTP_VEC_F32, TGTP_VEC_F32));
+                                     TGTP_VEC_F32, vec_store));
     }
 };
 
@@ -103,6 +116,7 @@ struct AESCConfig {
     std::string strFolder, strGraph;
     int omega = 0, gamma = 0;
     int precision = TGTP_PRECISION_FP32;
+    int vec_dtype = TGTP_VEC_F32;  // storage the mixed form reads (TGTP_VEC_F32 or TGTP_VEC_BF16)
 };
 
 // src/aesc.h:113-127
@@ -119,7 +133,7 @@ struct AESC {
         c.omega = config.omega;
         c.gamma = config.gamma;
         c.precision = config.precision;
-        c.vec_dtype = TGTP_VEC_F32;
+        c.vec_dtype = config.vec_dtype;
         check(tgtp_run(g.handle, &c, out.get()));
         return out.release();
     }

@@ -129,8 +129,9 @@ void* tgtp_graph_stream(tgtp_graph* g);
 tgtp_status tgtp_graph_info(const tgtp_graph* g, uint64_t* n, uint64_t* m);
 
 /* Uploads omega eigenpairs (values: double[omega]; vectors: vertex-major n*omega of `dtype`,
- * F32 or F64 host data).  F64 host data may be stored as F32 or BF16 on the device by passing
- * the host dtype in `dtype` and the device storage in `store_dtype`.  Several storages may be
+ * F32 or F64 host data).  The device storage may differ from the host type (F64 host data stored
+ * as F32 or BF16, F32 host data as BF16): pass the host dtype in `dtype` and the device storage in
+ * `store_dtype`.  Several storages may be
  * uploaded side by side; each call replaces the storage it names. */
 tgtp_status tgtp_eigens_upload(tgtp_graph* g, const double* values, const void* vectors,
                                uint32_t omega, int32_t dtype, int32_t store_dtype);

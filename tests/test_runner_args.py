@@ -125,3 +125,20 @@ def test_rw_experiment_saba_reports_an_unreadable_graph(runners, tmp_path):
     rc, out, err = _run(os.path.join(runners, "rw_experiment_saba"), ["nofolder", "ds", "5", "16"],
                         tmp_path)
     assert (rc, out, err) == (1, "", "rw_experiment_saba: cannot open graph: nofolder/ds/graph.txt")
+
+
+@pytest.mark.parametrize("name,args", [("tgtp", ["x", "y", "0.05", "16", "10", "o"]),
+                                       ("benchmark", ["ds", "0.05", "1", "1", "nofolder"])])
+@pytest.mark.parametrize("env,message", [
+    ({"TGTP_PRECISION": "fp16"}, "TGTP_PRECISION must be fp32, fp64 or mixed"),
+    ({"TGTP_VECTORS": "bf16"}, "TGTP_VECTORS=bf16 needs TGTP_PRECISION=mixed"),
+    ({"TGTP_VECTORS": "bf16", "TGTP_PRECISION": "fp64"}, "TGTP_VECTORS=bf16 needs TGTP_PRECISION=mixed"),
+    ({"TGTP_VECTORS": "fp8", "TGTP_PRECISION": "mixed"}, "TGTP_VECTORS must be f32 or bf16"),
+])
+def test_runner_form_variables_are_checked_before_loading(runners, tmp_path, name, args, env,
+                                                          message):
+    """The arithmetic form (TGTP_PRECISION) and the mixed form's vector storage (TGTP_VECTORS)
+    of the runners: a bad choice is reported before any input is read."""
+    r = subprocess.run([os.path.join(runners, name)] + args, capture_output=True, text=True,
+                       cwd=tmp_path, timeout=60, env=dict(os.environ, **env))
+    assert (r.returncode, r.stdout, r.stderr.strip()) == (1, "", f"{name}: {message}")

@@ -40,7 +40,8 @@ RUNNERS = {"tgtp": "tgtp_main.cpp", "benchmark": "benchmark_main.cpp",
 
 def _headers():
     return glob.glob(os.path.join(CSRC, "*.hpp")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(INCLUDE, "*.h")) + glob.glob(os.path.join(CSRC, "host", "*.hpp"))
+        glob.glob(os.path.join(INCLUDE, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.hpp")) + \
+        glob.glob(os.path.join(CSRC, "host", "*.hpp"))
 
 
 def _stale(target, deps):

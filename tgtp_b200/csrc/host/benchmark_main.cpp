@@ -73,6 +73,7 @@ void measure(const Plan& plan) {
     config.omega = plan.omega;
     config.gamma = plan.gamma;
     config.precision = precision_from_env();
+    config.vec_dtype = vectors_from_env(config.precision);
     std::vector<double> eps;
     for (const auto& e : plan.eps) {
         eps.push_back(tgtp_cli::bench_number(e));
@@ -83,7 +84,8 @@ void measure(const Plan& plan) {
 
     const auto dir = std::filesystem::path(plan.root) / plan.dataset;
     const auto eigens = dir / ("sorted_eigens_" + std::to_string(plan.omega) + ".txt");
-    AESCGraph graph((dir / "graph.txt").string(), eigens.string(), size_t(plan.omega), config.precision);
+    AESCGraph graph((dir / "graph.txt").string(), eigens.string(), size_t(plan.omega), config.precision,
+                    config.vec_dtype);
     config.delta = 1.0 / double(graph.n);
 
     std::cout << std::setprecision(10) << std::unitbuf;

@@ -5,7 +5,8 @@
 // Reads <folder>/<graph>/graph.txt and sorted_eigens_<omega>.txt, scores every CSR slot on the GPU
 // and writes the m scores as raw native-endian float32 in CSR order.  Exit 0, or 1 with
 // "tgtp: <message>" on stderr (argument errors as the reference words them, tgtp_cli).
-// Arithmetic form: TGTP_PRECISION=fp32 (default, the reference's arithmetic) | fp64 | mixed.
+// Arithmetic form: TGTP_PRECISION=fp32 (default, the reference's arithmetic) | fp64 | mixed; with
+// mixed, TGTP_VECTORS=bf16 stores the eigenvectors as BF16 (default f32).
 #include <climits>
 #include <filesystem>
 #include <fstream>
@@ -53,9 +54,11 @@ void score(const Job& job) {
     config.omega = job.omega;
     config.gamma = job.gamma;
     config.precision = precision_from_env();
+    config.vec_dtype = vectors_from_env(config.precision);
     const auto dir = std::filesystem::path(job.folder) / job.graph;
     const auto eigens = dir / ("sorted_eigens_" + std::to_string(job.omega) + ".txt");
-    AESCGraph graph((dir / "graph.txt").string(), eigens.string(), size_t(job.omega), config.precision);
+    AESCGraph graph((dir / "graph.txt").string(), eigens.string(), size_t(job.omega), config.precision,
+                    config.vec_dtype);
     config.delta = 1.0 / double(graph.n);
     // the output file is opened once the inputs have loaded, so an input error leaves no file
     std::ofstream sink(job.outfile, std::ios::binary);
