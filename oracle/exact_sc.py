@@ -48,9 +48,11 @@ def exact_scores(idx: np.ndarray, adj: np.ndarray) -> np.ndarray:
         iu, iv = np.nonzero(np.triu(block, 1))
         undirected_sum += float(np.sum(inv[iu, iu] + inv[iv, iv] - 2.0 * inv[iu, iv]))
     foster = abs(undirected_sum - (n - ncomp))
-    if not np.all(np.isfinite(out)) or residual > 1e-6 or foster > 1e-5 * max(1, n):
+    # an edge's effective resistance lies in [0, 1] (src/exact_sc.cpp:46 checks 1 + 1e-9)
+    in_range = bool(np.all((out >= -1e-12) & (out <= 1 + 1e-9)))
+    if not np.all(np.isfinite(out)) or residual > 1e-6 or foster > 1e-5 * max(1, n) or not in_range:
         raise RuntimeError(f"exact spanning centrality not certified: probe residual {residual:.3g}, "
-                           f"Foster deviation {foster:.3g}")
+                           f"Foster deviation {foster:.3g}, range ok {in_range}")
     return out
 
 
