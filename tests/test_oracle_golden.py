@@ -233,3 +233,16 @@ def test_exact_oracle_matches_the_reference_accuracy_script(manifest, name):
     got = exact_sc.exact_scores(c["idx"], c["adj"])
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) < 1e-12
+
+
+def test_oracle_does_not_depend_on_its_thread_count(manifest, oracle_lib):
+    """Like the reference (each source writes only its own row; walk seeds come from the grid),
+    the oracle's scores and SABA counters are the same bits on 1 and 4 threads."""
+    c = golden_tgtp_case(manifest, "cl300")
+    for fp64 in (False, True):
+        vec = c["v64"] if fp64 else c["v32"]
+        a = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], vec, 0.005, fp64=fp64, threads=1)
+        b = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], vec, 0.005, fp64=fp64, threads=4)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(oracle_lib.saba(c["idx"], c["adj"], 5, 64, threads=1),
+                          oracle_lib.saba(c["idx"], c["adj"], 5, 64, threads=4))
