@@ -191,6 +191,15 @@ def test_oracle_matches_the_reference_binary_at_omega_128(omega128_case, oracle_
     got64 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], eps, gamma=10, fp64=True)
     tol = np.maximum(1e-6 * np.abs(want), 2 * np.spacing(np.abs(want)))
     assert np.all(np.abs(got64.astype(np.float64) - want) <= tol)
+    # the paper's -Ofast build reassociates the omega sums: not bit-equal, within 1e-6 relative
+    fast_exe = os.path.join(ROOT, "oracle", "_ref", "tgtp")
+    if os.path.exists(fast_exe):
+        fast_out = c["root"] / f"scores_fast_{eps}.bin"
+        r = subprocess.run([fast_exe, str(c["root"]), "g", str(eps), "128", "10", str(fast_out)],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        fast = np.fromfile(fast_out, dtype=np.float32).astype(np.float64)
+        assert np.all(np.abs(got.astype(np.float64) - fast) <= 1e-6 * np.abs(fast))
 
 
 @pytest.mark.parametrize("graph,depth,walks", [("config1", 5, 2048), ("rmat14", 10, 64)])
