@@ -38,6 +38,17 @@ N_VERT, N_EDGES, EXPONENT, OMEGA, GAMMA, EPS = 4039, 88234, 2.5, 128, 10, 0.05
 WORKLOAD = ("tgtp AESC, plain FP64 form: Chung-Lu n=4039 E=88234 exp 2.5 (LCC), omega=128, "
             "gamma=10, eps=0.05")
 L2_FLUSH_BYTES = 256 << 20
+# push-bound companion workload: sparse Chung-Lu (28,000 ids, 120,000 target edges, exponent 2.1;
+# largest component n = 25,860, E = 119,972), where sources push for several rounds and walk
+SPARSE = dict(n0=28000, edges=120000, exponent=2.1, seed=1)
+PUSH_EPS = (0.01, 0.005)
+
+
+def bench_config(world: int) -> dict:
+    """The `config` both arms print (the same dict, so the two lines describe one workload)."""
+    return {"workload": WORKLOAD, "graph_seed": "1 + rank",
+            "l2": "GPU arm: flushed (256 MiB write) before every timed step; CPU arm: n/a",
+            "parallelism": f"replicas x{world}"}
 
 
 def peaks():
@@ -135,25 +146,27 @@ def cpu_model() -> str:
 def cpu_baseline_line(edges: int, secs_all, threads: int, secs_one, sample: str) -> dict:
     """cpu_baseline of the JSON line: the reference on all host cores (the value), the same on one
     core beside it, the core count, OMP_NUM_THREADS and the CPU model."""
-    out = {"value": edges / min(secs_all), "unit": "edges/s", "cores": threads,
+    out = {"value": edges / statistics.mean(secs_all), "unit": "edges/s", "cores": threads,
            "kind": "reference", "omp_num_threads": threads, "cpu_model": cpu_model(),
            "sample": sample}
     if secs_one:
-        out["single_thread"] = {"value": edges / min(secs_one), "unit": "edges/s", "cores": 1,
-                                "sample": "min of 3 tgtp() calls (after 1 warm-up), "
-                                          "OMP_NUM_THREADS=1"}
+        out["single_thread"] = {"value": edges / statistics.mean(secs_one), "unit": "edges/s",
+                                "cores": 1, "sample": "mean of 3 tgtp() calls (after 1 warm-up), "
+                                                      "OMP_NUM_THREADS=1"}
     return out
 
 
-def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int, warmups: int):
-    """The reference's own benchmark binary (compiled from its sources into oracle/_ref)."""
+def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int, warmups: int,
+                      eps: float = EPS):
+    """Seconds of each timed tgtp() call of the reference's own benchmark binary (compiled from its
+    sources into oracle/_ref), or None when it was not built."""
     import oracle
 
     exe = oracle.ref_binary("benchmark")
     if exe is None:
         return None
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    r = subprocess.run([exe, dataset, str(EPS), str(threads), str(repeats), folder_root,
+    r = subprocess.run([exe, dataset, str(eps), str(threads), str(repeats), folder_root,
                         str(OMEGA), str(GAMMA), str(warmups)], capture_output=True, text=True,
                        env=env, timeout=1800)
     if r.returncode != 0:
@@ -187,10 +200,11 @@ def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3):
         # already counts every hop (n * n_walks * depth): transitions
         f = r.stdout.strip().splitlines()[-1].split("\t")
         walk_s.append((float(f[8]), float(f[10])))
-    t_rw, total = min(walk_s)
+    t_rw = statistics.mean(t for t, _ in walk_s)
+    total = walk_s[0][1]
     return {"transitions_per_s": total / t_rw, "transitions": total, "cores": threads,
             "omp_num_threads": threads, "walk_seconds": t_rw,
-            "sample": f"min of {runs} runs of the reference rw_experiment_saba (-Ofast, OpenMP) "
+            "sample": f"mean of {runs} runs of the reference rw_experiment_saba (-Ofast, OpenMP) "
                       "on the same graph"}
 
 
@@ -225,6 +239,116 @@ def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
         if ref is not None:
             out["cpu_reference"] = ref
     return out
+
+
+def source_bytes(st: dict, taus, idx) -> tuple[int, int]:
+    """Algorithmic bytes of the per-source stage (source_kernel and, in the mixed form's block
+    mode, push_block) of one run: 20 B per push traversal (adjacency 4, the vertex's offset pair 8,
+    residual read-modify-write 8) + 12 B per frontier vertex + 32 B per two-walker hop, without the
+    rows that finish in closed form (every tau <= 1: finish_kernel scores them, and the run counters
+    include their one round).  Returns (bytes, closed-form traversals)."""
+    import numpy as np
+
+    deg = np.diff(idx.astype(np.int64))
+    row_max = np.maximum.reduceat(taus, idx[:-1].astype(np.int64)) if len(taus) else taus
+    closed = row_max <= 1
+    closed_trav = int(deg[closed].sum())
+    closed_rows = int(closed.sum())
+    trav = st["push_traversals"] - closed_trav
+    pv = st["push_vertices"] - closed_rows
+    return 20 * trav + 12 * pv + 32 * st["walk_hops"], closed_trav
+
+
+def push_bound_section(dg, idx, E, folder_root, dataset, eps_list, stream, out, flush, hbm,
+                       peak_kind, steps, with_cpu, flush_l2=True):
+    """tgtp() where the work is: epsilon values at which sources push past their first round and
+    slots walk.  Per epsilon and form: edges/s and ms per step (CUDA events on the launching stream,
+    `steps` timed runs after 2 warm-up, L2 flushed before each), the work counters, the per-source
+    stage's share and its algorithmic bytes / event-timed time against the HBM peak; beside them the
+    reference's benchmark binary on the same graph and eigen files (mean of 2 calls after 1 warm-up
+    on all host cores)."""
+    import torch
+
+    from tgtp_b200.aesc import (AESC, AESCConfig, PRECISION_FP64, PRECISION_MIXED, VEC_BF16,
+                                VEC_F32)
+
+    forms = (("fp64", PRECISION_FP64, VEC_F32), ("mixed_f32_vectors", PRECISION_MIXED, VEC_F32),
+             ("mixed_bf16_vectors", PRECISION_MIXED, VEC_BF16))
+    res = {}
+    for eps in eps_list:
+        cell = {}
+        for label, prec, vec in forms:
+            a = AESC(dg, AESCConfig(eps, omega=OMEGA, gamma=GAMMA, precision=prec, vec_dtype=vec))
+            for _ in range(2):
+                a.tgtp_device(out.data_ptr())
+            torch.cuda.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(steps)]
+            for e0, e1 in ev:
+                if flush_l2:
+                    flush.zero_()
+                e0.record(stream)
+                a.tgtp_device(out.data_ptr())
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+            st = a.stats()
+            taus = a.taus()
+            dg.set_profiling(True)
+            a.tgtp_device(out.data_ptr())
+            ks = dg.kernel_stats()
+            dg.set_profiling(False)
+            src_ms = sum(v[1] for k, v in ks.items() if k in ("source", "push_block", "row_key"))
+            tot_ms = sum(v[1] for v in ks.values())
+            sbytes, closed_trav = source_bytes(st, taus, idx)
+            achieved = sbytes / (src_ms * 1e-3) / 1e9 if src_ms > 0 else None
+            cell[label] = {
+                "edges_per_s": E / (ms * 1e-3), "ms_per_step": ms,
+                "counters": {k: st[k] for k in ("push_rounds", "push_vertices", "push_traversals",
+                                                "walk_edges", "walk_count", "walk_hops")},
+                "kernel_ms": {k: v[1] / v[0] for k, v in ks.items()},
+                "per_source_stage": {"kernels": "source (+ push_block, row_key)",
+                                     "share": src_ms / tot_ms if tot_ms else None,
+                                     "algorithmic_bytes": sbytes,
+                                     "closed_form_traversals_excluded": closed_trav,
+                                     "achieved_gbs": achieved,
+                                     "frac_of_" + peak_kind + "_hbm":
+                                         achieved / hbm if achieved else None},
+            }
+            if label == "fp64":
+                fp64_out = out.double().clone()
+            else:
+                dev = (out.double() - fp64_out).abs() / fp64_out.abs()
+                cell[label]["rel_dev_vs_fp64"] = {"median": float(dev.median()),
+                                                  "p99": float(torch.quantile(dev.float(), 0.99)),
+                                                  "max": float(dev.max())}
+                cell[label]["speedup_vs_fp64"] = cell["fp64"]["ms_per_step"] / ms
+        if with_cpu:
+            threads = os.cpu_count() or 1
+            secs = cpu_reference_run(folder_root, dataset, threads, 2, 1, eps)
+            if secs:
+                cell["cpu_reference"] = {"edges_per_s": E / statistics.mean(secs),
+                                         "seconds": statistics.mean(secs), "cores": threads,
+                                         "omp_num_threads": threads,
+                                         "sample": "mean of 2 tgtp() calls after 1 warm-up, "
+                                                   "reference benchmark binary"}
+        res[f"eps_{eps}"] = cell
+    return res
+
+
+def sparse_inputs(root: str):
+    """The sparse Chung-Lu companion graph with its 128 eigenpairs (scipy restatement of the eigen
+    prep), written and parsed back like the reference's files."""
+    from tgtp_b200 import eigenprep, synth
+    from tgtp_b200.aesc import load_eigens_txt
+
+    g = synth.chung_lu(SPARSE["n0"], SPARSE["edges"], SPARSE["exponent"], SPARSE["seed"])
+    folder = os.path.join(root, "sparse")
+    os.makedirs(folder, exist_ok=True)
+    synth.write_graph_txt(g, os.path.join(folder, "graph.txt"))
+    epath = eigenprep.eigenprep_folder(folder, OMEGA)
+    values, v32, v64 = load_eigens_txt(epath, g.n, OMEGA)
+    return g, values, v32, v64
 
 
 def run_batch_workload(args):
@@ -363,7 +487,7 @@ def run_reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Chung-Lu + scipy eigenpairs)",
-        "config": {"workload": WORKLOAD, "graph_seed": 1, "l2": "n/a (CPU)"},
+        "config": bench_config(args.gpus),
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "reference",
                          "omp_num_threads": threads, "cpu_model": cpu_model(),
                          "sample": f"{args.steps} timed tgtp() calls after {args.warmup} warm-up, "
@@ -384,6 +508,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmat", action="store_true", help="skip the R-MAT scale-18 walk line")
+    ap.add_argument("--no-push", action="store_true",
+                    help="skip the push-bound tgtp measurements (eps 0.01 / 0.005, sparse graph)")
     ap.add_argument("--workload", choices=["aesc", "batch"], default="aesc",
                     help="batch: the 64-graph batched workload instead of the headline")
     args = ap.parse_args()
@@ -555,6 +681,28 @@ def main():
         if not args.no_rmat:
             saba["rmat18"] = saba_rmat18(hbm, peak_kind, root, not args.no_cpu_baseline)
 
+        # ---- tgtp where the push and the walks run ----
+        push = {}
+        if not args.no_push:
+            push["chunglu4039"] = push_bound_section(
+                dg, idx, E, root, "cl4039", PUSH_EPS, stream, out, flush, hbm, peak_kind, 10,
+                not args.no_cpu_baseline)
+            sg, svals, sv32, sv64 = sparse_inputs(root)
+            sidx, sadj = sg.csr()
+            sdg = AESCGraph.from_csr(sidx, sadj)
+            sdg.set_stream(stream.cuda_stream)
+            sdg.upload_eigens(svals, sv64, VEC_F64)
+            sdg.upload_eigens(svals, sv32, VEC_F32)
+            sdg.upload_eigens(svals, sv32, VEC_BF16)
+            sout = torch.empty(int(sidx[-1]), dtype=torch.float32, device="cuda")
+            push["sparse_chunglu"] = {
+                "graph": f"Chung-Lu {SPARSE['n0']} ids, {SPARSE['edges']} target edges, exponent "
+                         f"{SPARSE['exponent']}, seed {SPARSE['seed']}, largest component: "
+                         f"n={sg.n}, E={sg.num_edges}; omega=128, gamma=10",
+                **push_bound_section(sdg, sidx, sg.num_edges, root, "sparse", (0.005,), stream,
+                                     sout, flush, hbm, peak_kind, 3, not args.no_cpu_baseline)}
+            sdg.free()
+
         cpu = None
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -562,16 +710,14 @@ def main():
             if secs:
                 one = cpu_reference_run(root, "cl4039", 1, 3, 1)
                 cpu = cpu_baseline_line(E, secs, threads, one,
-                                        "min of 5 tgtp() calls (after 1 warm-up) of the reference "
+                                        "mean of 5 tgtp() calls (after 1 warm-up) of the reference "
                                         "benchmark binary on the same graph and eigen files")
         line = {
             "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Chung-Lu graph + scipy eigenpairs)",
-            "config": {"workload": WORKLOAD, "graph_seed": "1 + rank",
-                       "l2": "flushed (256 MiB write) before every timed step",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(world),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": per_launch[top]},
@@ -591,6 +737,7 @@ def main():
                                  speedup_vs_fp64=ms_step / v["ms_per_step"])
                          for k, v in mixed.items()}},
             "saba": saba,
+            "push_bound": push,
             "wall_s_timed_region": wall64,
         }
         print(json.dumps(line))

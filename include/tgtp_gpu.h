@@ -187,14 +187,17 @@ tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
 /* No counterpart in the reference: the walk counter for callers that cannot allocate device
  * memory, e.g. a process whose device memory is owned by another allocator or budget, or a
  * latency-critical loop where cudaMalloc/cudaFree would synchronise the device.  It allocates
- * nothing: the caller passes the CSR already on the device (n + 1 offsets, m neighbours) and gets
- * the walk runner's summary.  The per-vertex counters and sums live in one fixed 16 MiB device
- * array inside the library, present on every GPU that loads it until the process exits, so n is
- * limited to 4,194,304 vertices (larger n is rejected with TGTP_ERR_INVALID_ARGUMENT).  The first
- * call on a device looks up that array's address; make that first call before any stream capture.
+ * nothing: the caller passes the CSR already on the device (n + 1 offsets, and device_adj holding
+ * the idx[n] neighbours the offsets declare) and gets the walk runner's summary.  The per-vertex
+ * counters and sums live in one fixed 16 MiB device array inside the library, present on every
+ * GPU that loads it until the process exits, so n is limited to 4,194,304 vertices (larger n is
+ * rejected with TGTP_ERR_INVALID_ARGUMENT).  Before any walk the CSR is checked on the device:
+ * offsets starting at 0 and never decreasing, neighbour ids below n, and no edge into a vertex
+ * without neighbours; a CSR that fails is refused with TGTP_ERR_INVALID_ARGUMENT and no walk runs.
  * Every call clears and reuses the same array: calls that overlap on the GPU (other streams,
  * other threads) race and give wrong results.  Runs on cuda_stream (NULL: the default stream) and
- * returns after synchronising it. */
+ * synchronises it (twice: after the check and at the end), so it cannot be called while that
+ * stream is being captured into a CUDA graph. */
 tgtp_status saba_count_static(const uint32_t* device_idx, const uint32_t* device_adj, uint64_t n,
                               uint32_t depth, uint32_t n_walks, void* cuda_stream,
                               saba_result* out);

@@ -17,7 +17,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_SRC = "/root/reference/src"
+# The reference checkout (ggokturk/tgtp); TGTP_REFERENCE overrides the default location.
+REFERENCE = os.environ.get("TGTP_REFERENCE", "/root/reference")
+REFERENCE_SRC = os.path.join(REFERENCE, "src")
 
 _lib = None
 
@@ -35,7 +37,7 @@ def build(reference: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources exist here, oracle/_ref/*."""
     subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
     if reference and os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j4"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j4", "REF=" + REFERENCE], check=True)
 
 
 def ref_binary(name: str) -> str | None:

@@ -15,6 +15,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+if GOLDEN not in sys.path:
+    sys.path.insert(0, GOLDEN)  # the fixture generators' helpers (hashes, fingerprints)
 
 
 def pytest_configure(config):
@@ -89,4 +91,4 @@ def config1_inputs():
     path = eigenprep.eigenprep_folder(d, 128)
     idx, adj = g.csr()
     values, v32, v64 = load_eigens_txt(path, g.n, 128)
-    return dict(idx=idx, adj=adj, values=values, v32=v32, v64=v64, n=g.n)
+    return dict(idx=idx, adj=adj, values=values, v32=v32, v64=v64, n=g.n, folder=d)

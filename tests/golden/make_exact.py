@@ -2,7 +2,7 @@
 by the reference's own accuracy script (scripts/paper_accuracy.py, exact_scores), imported from the
 reference sources in this container.  One float64 array per graph, in CSR slot order.
 
-Run here (needs /root/reference):
+Run where the reference checkout is present (TGTP_REFERENCE, default /root/reference):
     python tests/golden/make_exact.py
 """
 from __future__ import annotations
@@ -15,7 +15,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SCRIPT = "/root/reference/scripts/paper_accuracy.py"
+SCRIPT = os.path.join(os.environ.get("TGTP_REFERENCE", "/root/reference"), "scripts",
+                      "paper_accuracy.py")
 CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12"]
 
 

@@ -10,7 +10,8 @@ from its sources (oracle/Makefile -> oracle/_ref/):
               straight to float differs from parsing to double and rounding.
 Graphs and eigenpairs are seeded synthetic inputs (tgtp_b200.synth, tgtp_b200.eigenprep).
 
-Run here (needs /root/reference and the oracle/_ref binaries):
+Run where the reference checkout is present (TGTP_REFERENCE, default /root/reference) and the
+oracle/_ref binaries are built from it:
     python tests/golden/make_golden.py
 """
 from __future__ import annotations

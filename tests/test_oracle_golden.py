@@ -255,3 +255,30 @@ def test_oracle_does_not_depend_on_its_thread_count(manifest, oracle_lib):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert np.array_equal(oracle_lib.saba(c["idx"], c["adj"], 5, 64, threads=1),
                           oracle_lib.saba(c["idx"], c["adj"], 5, 64, threads=4))
+
+
+def test_saba_rmat18_fixture_is_reproduced_by_the_oracle(oracle_lib):
+    """tests/golden/saba_rmat18.json (the R-MAT scale-18 walk counters the GPU tests compare with):
+    the graph generator still gives the graph it was made on, every cell's visit count is n * W * D,
+    and the oracle reproduces the benchmark cell (depth 5, 2,048 walks) hash for hash, the cell
+    where the fixture holds the reference's own counters."""
+    import json
+
+    from make_saba_rmat18 import CELLS, graph_fingerprint, sha256_u32
+
+    from tgtp_b200 import synth
+
+    with open(os.path.join(GOLDEN, "saba_rmat18.json")) as f:
+        fx = json.load(f)
+    g = synth.config3_graph(1)
+    idx, adj = g.csr()
+    assert graph_fingerprint(idx, adj) == fx["fingerprint"]
+    assert sorted((c["depth"], c["n_walks"]) for c in fx["cells"]) == sorted(CELLS)
+    for c in fx["cells"]:
+        assert c["visit_count"] == g.n * c["n_walks"] * c["depth"]
+        assert c["max_counter"] < 2**32
+    cell = [c for c in fx["cells"] if (c["depth"], c["n_walks"]) == (5, 2048)][0]
+    assert cell["source"].startswith("reference")
+    got = oracle_lib.saba(idx, adj, 5, 2048)
+    assert sha256_u32(got) == cell["counters_sha256"]
+    assert int((got * np.arange(1, g.n + 1, dtype=np.uint64)).sum()) == cell["checksum"]

@@ -409,41 +409,56 @@ namespace {
 // Largest vertex count saba_count_static accepts (16 MiB of uint32 counters).
 constexpr uint64_t kStaticSabaMaxVertices = uint64_t(1) << 22;
 // Words 0..7: four uint64 sums (visit count, checksum, fallback bouquets, active vertices);
-// counters start at word 64 (byte 256).
+// word 8: the CSR check's flags (kBad* below); counters start at word 64 (byte 256).
 constexpr uint64_t kStaticSabaHeaderWords = 64;
+constexpr uint64_t kStaticSabaFlagWord = 8;
+enum : uint32_t { kBadOffsets = 1u, kBadNeighbour = 2u, kDeadEnd = 4u };
 
 __device__ __align__(256) uint32_t g_static_saba_scratch[kStaticSabaHeaderWords + kStaticSabaMaxVertices];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mu;
-void* g_static_addr[kMaxDevices] = {};
-int g_static_sms[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device.  It is looked up on every call
+// (cudaGetSymbolAddress allocates nothing and is cheap), so a new primary context after a
+// cudaDeviceReset never sees a stale address.
 void* static_scratch(int device, int* num_sms) {
-    if (device < 0 || device >= kMaxDevices) fail(TGTP_ERR_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[device]) {
-        void* p = nullptr;
-        TGTP_CUDA(cudaGetSymbolAddress(&p, g_static_saba_scratch));
-        int sms = 0;
-        TGTP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        g_static_sms[device] = sms;
-        g_static_addr[device] = p;
-    }
-    *num_sms = g_static_sms[device];
-    return g_static_addr[device];
+    void* p = nullptr;
+    TGTP_CUDA(cudaGetSymbolAddress(&p, g_static_saba_scratch));
+    TGTP_CUDA(cudaDeviceGetAttribute(num_sms, cudaDevAttrMultiProcessorCount, device));
+    return p;
 }
 
-__global__ void static_active_kernel(const uint32_t* __restrict__ idx, uint64_t n,
-                                     unsigned long long* __restrict__ active) {
+// The caller's CSR is checked before any walk: offsets start at 0 and never decrease, every
+// neighbour id is below n, and every neighbour has a nonzero degree (a walk that reached a vertex
+// without neighbours would pick adj[idx[cur] + (r % 0)]).  Offsets are checked by one pass; the
+// neighbour pass reads adj[0 .. idx[n]) only, the slots the CSR declares.  Violations set flag bits
+// in the scratch header; the host reads them back and refuses the call.
+__global__ void static_check_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ adj,
+                                    uint64_t n, uint32_t* __restrict__ flags,
+                                    unsigned long long* __restrict__ active) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    uint32_t bad = 0;
     unsigned long long a = 0;
-    for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
-         v += uint64_t(gridDim.x) * blockDim.x)
-        a += idx[v + 1] != idx[v];
+    if (t0 == 0 && idx[0] != 0u) bad |= kBadOffsets;
+    for (uint64_t v = t0; v < n; v += stride) {
+        const uint32_t b = idx[v], e = idx[v + 1];
+        if (e < b) bad |= kBadOffsets;
+        a += e != b;
+    }
+    const uint64_t m = idx[n];
+    for (uint64_t q = t0; q < m; q += stride) {
+        const uint32_t u = adj[q];
+        if (uint64_t(u) >= n) bad |= kBadNeighbour;
+        else if (idx[u + 1] == idx[u]) bad |= kDeadEnd;
+    }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(kFullMask, a, o);
-    if ((threadIdx.x & 31) == 0 && a) atomicAdd(active, a);
+    for (int o = 16; o; o >>= 1) {
+        a += __shfl_xor_sync(kFullMask, a, o);
+        bad |= __shfl_xor_sync(kFullMask, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (a) atomicAdd(active, a);
+        if (bad) atomicOr(flags, bad);
+    }
 }
 
 }  // namespace
@@ -472,9 +487,20 @@ extern "C" tgtp_status saba_count_static(const uint32_t* device_idx, const uint3
         cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
         // the array keeps the previous call's contents: start from zero
         TGTP_CUDA(cudaMemsetAsync(base, 0, sizeof(uint32_t) * (kStaticSabaHeaderWords + n), s));
-        static_active_kernel<<<unsigned(std::min<uint64_t>((n + 255) / 256, 4u * num_sms)), 256, 0, s>>>(
-            device_idx, n, sums + 3);
-        TGTP_LAUNCH_CHECK("static_active_kernel");
+        static_check_kernel<<<unsigned(std::min<uint64_t>((n + 255) / 256, 4u * num_sms)), 256, 0, s>>>(
+            device_idx, device_adj, n, base + kStaticSabaFlagWord, sums + 3);
+        TGTP_LAUNCH_CHECK("static_check_kernel");
+        uint32_t flags = 0;
+        TGTP_CUDA(cudaMemcpyAsync(&flags, base + kStaticSabaFlagWord, sizeof(flags),
+                                  cudaMemcpyDeviceToHost, s));
+        TGTP_CUDA(cudaStreamSynchronize(s));
+        if (flags & kBadOffsets)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "CSR offsets must start at 0 and never decrease");
+        if (flags & kBadNeighbour)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "CSR neighbour id out of range (must be below n)");
+        if (flags & kDeadEnd)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "CSR has an edge into a vertex without neighbours (a walk could not leave it)");
         if (n_walks && depth) {
             const uint32_t bouquets_per_src = n_walks / 8;
             const uint32_t grid_step = UINT32_MAX / n_walks;
