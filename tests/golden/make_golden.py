@@ -12,7 +12,8 @@ Graphs and eigenpairs are seeded synthetic inputs (tgtp_b200.synth, tgtp_b200.ei
 
 Run where the reference checkout is present (TGTP_REFERENCE, default /root/reference) and the
 oracle/_ref binaries are built from it:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                    # every case
+    python tests/golden/make_golden.py --cases multi300   # only the named multigraph tgtp cases
 """
 from __future__ import annotations
 
@@ -77,6 +78,28 @@ TGTP_CASES = {
     "complete12": (lambda: complete(12), 6, [(0.05, 10), (0.005, 10)]),
 }
 
+
+
+def multigraph_text() -> str:
+    """The cl300 graph with 12 of its edges listed again and 5 self-loops: the loader keeps both
+    (src/graph.h:63-66, 75-78), so rows repeat neighbours and hold their own vertex."""
+    g = synth.chung_lu(300, 2000, 2.5, 11)
+    rng = np.random.default_rng(17)
+    lines = [f"{a} {b}" for a, b in zip(g.u.tolist(), g.v.tolist())]
+    for e in rng.choice(len(lines), 12, replace=False):
+        lines.append(lines[e])
+    for v in rng.choice(g.n, 5, replace=False):
+        lines.append(f"{v} {v}")
+    return "\n".join(lines) + "\n"
+
+
+# multigraph cases: (text of graph.txt, eigenpairs of this simple graph, omega, runs); the
+# eigenpairs are inputs only, so they come from the simple graph the text extends
+TGTP_RAW = {
+    "multi300": (multigraph_text, lambda: synth.chung_lu(300, 2000, 2.5, 11), 16,
+                 [(0.05, 10), (0.01, 10), (0.005, 10), (0.01, 1)]),
+}
+
 LOADER_CASES = {
     "comments": "# header\n% other\n0 1\n\n   \n  # indented comment\n1 2 extra tokens\n2 0\r\n",
     "selfloop_dup": "0 1\n1 1\n0 1\n1 2\n2 0\n",
@@ -93,10 +116,48 @@ def run(cmd, **kw):
     return subprocess.run(cmd, check=True, capture_output=True, text=True, **kw)
 
 
+def tgtp_runs(name, folder, omega, n, runs, manifest):
+    """The reference's tgtp (-O2) on folder/graph.txt for each (eps, gamma); scores saved as .npy."""
+    for eps, gamma in runs:
+        out = os.path.join(folder, f"scores_eps{eps}_g{gamma}.f32")
+        run([os.path.join(REF, "tgtp_O2"), os.path.join(HERE, "tgtp"), name, str(eps),
+             str(omega), str(gamma), out], env=dict(os.environ, OMP_NUM_THREADS="2"))
+        s = np.fromfile(out, dtype=np.float32)
+        os.remove(out)
+        np.save(out.replace(".f32", ".npy"), s)
+        manifest["tgtp"].append(dict(case=name, omega=omega, epsilon=eps, gamma=gamma,
+                                     n=int(n), m=int(s.size),
+                                     scores=os.path.join(name, os.path.basename(
+                                         out.replace(".f32", ".npy")))))
+
+
+def raw_tgtp_case(name, manifest):
+    text, simple, omega, runs = TGTP_RAW[name]
+    folder = os.path.join(HERE, "tgtp", name)
+    shutil.rmtree(folder, ignore_errors=True)
+    os.makedirs(folder)
+    with open(os.path.join(folder, "graph.txt"), "w") as f:
+        f.write(text())
+    g = simple()
+    vals, vecs, m = eigenprep.compute(g.n, g.u, g.v, omega, seed=0)
+    eigenprep.write_files(folder, g.n, m, vals, vecs)
+    tgtp_runs(name, folder, omega, g.n, runs, manifest)
+
+
 def main():
     for need in ("tgtp_O2", "saba_harness_O2", "ref_load_dump"):
         if not os.access(os.path.join(REF, need), os.X_OK):
             sys.exit(f"missing {REF}/{need}: run `make -C oracle ref` first")
+    if len(sys.argv) > 2 and sys.argv[1] == "--cases":
+        # (re)make only the named multigraph tgtp cases, keeping the rest of the manifest
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            manifest = json.load(f)
+        for name in sys.argv[2].split(","):
+            manifest["tgtp"] = [r for r in manifest["tgtp"] if r["case"] != name]
+            raw_tgtp_case(name, manifest)
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(manifest, f, indent=1)
+        return
     for sub in ("saba", "tgtp", "loader", "eigens"):
         shutil.rmtree(os.path.join(HERE, sub), ignore_errors=True)
         os.makedirs(os.path.join(HERE, sub))
@@ -132,17 +193,9 @@ def main():
         n, u, v = eigenprep.read_edges(os.path.join(folder, "graph.txt"))
         vals, vecs, m = eigenprep.compute(n, u, v, omega, seed=0)
         eigenprep.write_files(folder, n, m, vals, vecs)
-        for eps, gamma in runs:
-            out = os.path.join(folder, f"scores_eps{eps}_g{gamma}.f32")
-            run([os.path.join(REF, "tgtp_O2"), os.path.join(HERE, "tgtp"), name, str(eps),
-                 str(omega), str(gamma), out], env=dict(os.environ, OMP_NUM_THREADS="2"))
-            s = np.fromfile(out, dtype=np.float32)
-            os.remove(out)
-            np.save(out.replace(".f32", ".npy"), s)
-            manifest["tgtp"].append(dict(case=name, omega=omega, epsilon=eps, gamma=gamma,
-                                         n=int(n), m=int(s.size),
-                                         scores=os.path.join(name, os.path.basename(
-                                             out.replace(".f32", ".npy")))))
+        tgtp_runs(name, folder, omega, n, runs, manifest)
+    for name in TGTP_RAW:
+        raw_tgtp_case(name, manifest)
 
     # ---- loader ----
     for name, text in LOADER_CASES.items():

@@ -40,6 +40,13 @@ def test_reference_arm_prints_the_contract_line():
     assert d["e2e"] == {"value": d["value"], "unit": "edges/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]
+    # both arms print the same config dict (bench.bench_config), so they describe one workload
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert d["config"] == bench.bench_config(1)
 
 
 def test_reference_arm_runs_on_rank_zero_only():
@@ -52,9 +59,11 @@ def test_cpu_baseline_line_reports_both_thread_counts():
     spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
-    line = bench.cpu_baseline_line(1000, [0.5, 0.25], 16, [2.0, 4.0], "sample")
-    assert line["value"] == 4000 and line["cores"] == 16 and line["omp_num_threads"] == 16
-    assert line["single_thread"]["value"] == 500 and line["single_thread"]["cores"] == 1
+    # one sampling rule for the reference arm and cpu_baseline: the mean of the timed calls
+    line = bench.cpu_baseline_line(1000, [0.5, 0.25, 0.25], 16, [2.0, 4.0], "sample")
+    assert line["value"] == 1000 / (1.0 / 3.0) and line["cores"] == 16
+    assert line["omp_num_threads"] == 16
+    assert line["single_thread"]["value"] == 1000 / 3.0 and line["single_thread"]["cores"] == 1
     assert line["cpu_model"] and line["kind"] == "reference"
     assert "single_thread" not in bench.cpu_baseline_line(1000, [0.5], 16, None, "sample")
 

@@ -9,7 +9,10 @@ import pytest
 
 from conftest import GOLDEN, golden_tgtp_case, load_golden_scores
 
-TGTP_CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12"]
+SIMPLE_CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12"]
+# multi300 repeats edges and holds self-loops: its scores are not symmetric slot by slot (only the
+# last repeat's value lands on the reverse slot, src/aesc.h:538-545) and it has no exact fixture
+TGTP_CASES = SIMPLE_CASES + ["multi300"]
 
 
 def _csr_from_graph(path):
@@ -54,7 +57,7 @@ def test_tgtp_oracle_fp64_close_to_reference(manifest, oracle_lib, tgtp_lib, nam
         assert bad.mean() <= 0.01, (run, int(bad.sum()))
 
 
-@pytest.mark.parametrize("name", TGTP_CASES)
+@pytest.mark.parametrize("name", SIMPLE_CASES)
 def test_reference_scores_are_symmetric_and_sane(manifest, tgtp_lib, name):
     c = golden_tgtp_case(manifest, name)
     idx, adj = c["idx"], c["adj"]
@@ -231,7 +234,7 @@ def test_saba_oracle_matches_the_reference_walks_at_benchmark_size(tmp_path, ora
     assert checksum == int((got * np.arange(1, n + 1, dtype=np.uint64)).sum())
 
 
-@pytest.mark.parametrize("name", TGTP_CASES)
+@pytest.mark.parametrize("name", SIMPLE_CASES)
 def test_exact_oracle_matches_the_reference_accuracy_script(manifest, name):
     """oracle/exact_sc.py against the exact scores of the reference's scripts/paper_accuracy.py
     (tests/golden/exact/, made by tests/golden/make_exact.py) on the golden graphs."""

@@ -13,7 +13,8 @@ from conftest import golden_tgtp_case, load_golden_scores
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12"]
+# multi300: the cl300 graph with repeated edges and self-loops, which the reference's loader keeps
+CASES = ["cl300", "sparse400", "grid", "cycle9", "complete12", "multi300"]
 STAT_KEYS = ["push_rounds", "push_vertices", "push_traversals", "walk_edges", "walk_count",
              "walk_hops", "fallback_bouquets", "tau_iterations"]
 
@@ -155,6 +156,27 @@ def test_config2_fp64_matches_oracle_bitwise_and_the_reference_on_every_slot(
     assert ref.shape == got.shape
     bad = _outside_reference_tolerance(got, ref)
     assert bad.size == 0, (bad[:8], got[bad[:4]], ref[bad[:4]])
+
+
+def test_multigraph_taus_leave_the_unwritten_repeats_at_zero(manifest, cuda_device, oracle_lib):
+    """In a row that repeats a smaller neighbour, the reference writes tau only into the first of
+    the repeats (lower_bound, src/aesc.h:207-209) and leaves the others 0; the GPU run does the
+    same, and the mixed form refuses such a graph (TGTP_ERR_UNSUPPORTED) instead of guessing."""
+    from tgtp_b200.aesc import (AESC, AESCConfig, PRECISION_MIXED, TgtpError, VEC_F32)
+
+    c = golden_tgtp_case(manifest, "multi300")
+    g = _device_graph(c)
+    a = AESC(g, AESCConfig(0.01, omega=c["omega"]))
+    a.tgtp()
+    taus = a.taus()
+    _, det = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v32"], 0.01, details=True)
+    assert np.array_equal(taus, det["taus"])
+    assert (taus == 0).sum() == 12  # the 12 repeated edges' later slots in the larger end's row
+    with pytest.raises(TgtpError) as e:
+        AESC(g, AESCConfig(0.01, omega=c["omega"], precision=PRECISION_MIXED,
+                           vec_dtype=VEC_F32)).tgtp()
+    assert e.value.status == 6
+    g.free()
 
 
 def test_invalid_arguments_are_rejected(manifest, cuda_device):

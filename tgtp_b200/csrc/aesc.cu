@@ -18,7 +18,8 @@
 // The parity forms (FP32 = the reference's own arithmetic, FP64 = every real held in double)
 // keep the reference's evaluation order wherever a rounding depends on it:
 //   * the push of one source is sequential over its frontier, in discovery order; the lanes of the
-//     warp share one frontier vertex's adjacency (distinct neighbours, so their updates commute);
+//     warp share one frontier vertex's adjacency (distinct neighbours update distinct words; a run
+//     of one repeated neighbour is applied by its first lane, one add per repeat, in order);
 //   * float sums run in the reference's order (walk lanes per bouquet lane in bouquet order, the
 //     eight lanes summed 0..7; the FP32 form's tau dot products per edge in index order, the FP64
 //     form's in its fixed eight-way split);
@@ -950,6 +951,10 @@ struct SourceParams {
     const PrePush* pre;
     const float* pre_cols;
     const uint32_t* pre_final;
+    // The graph has rows that repeat a neighbour or hold their own vertex (the reference's loader
+    // keeps duplicate edges and self-loops, src/graph.h:63-66, 75-78): the first round takes the
+    // general path and the push serialises each run of a repeated neighbour (parity forms only).
+    bool multi;
 };
 
 template <class Real>
@@ -1541,8 +1546,43 @@ source_kernel(SourceParams<Real, Acc> p) {
             // The frontier is {src} with residual 1 (pvec[src] = 1.0, then zeroed as it is drained):
             // every neighbour u is discovered in row order and receives 0 + 1/deg(u) = 1/deg(u), so
             // the round's new frontier, residuals, degree sum, max / min and row update
-            // preds = 1/ds + (0 - 1/deg(u)) / ds follow from one pass over the row.  Neighbours are
-            // distinct (tgtp_run rejects repeated neighbours and self-loops).
+            // preds = 1/ds + (0 - 1/deg(u)) / ds follow from one pass over the row when the
+            // neighbours are distinct.  Rows of a graph with repeated neighbours or self-loops
+            // (p.multi, parity forms) take the general path below instead.
+            if (!JACOBI && p.multi) {
+                // (1) each run of one neighbour u (rows are sorted, so repeats are adjacent) is
+                // handled by its first slot: k repeats add 1/deg(u) k times in order, as the
+                // reference's sequential += does; that slot discovers u (first-occurrence order)
+                // and adds deg(u) to picost.  pvec[src] starts at 0 (it was drained), so a
+                // self-loop run adds to it like to any neighbour.
+                uint32_t found = 0;
+                for (uint32_t c = 0; c < dsi; c += 32) {
+                    const uint32_t o = c + lane;
+                    const bool in = o < dsi;
+                    const uint2 a = in ? __ldg(p.adjd + rb + o) : make_uint2(NONE, 1u);
+                    const bool lead = in && (o == 0 || __ldg(adj + rb + o - 1) != a.x);
+                    Real pu = Real(0);
+                    if (lead) {
+                        const Real x = rdiv(Real(1), from_u64<Real>(a.y));
+                        pu = x;
+                        for (uint32_t k = o + 1; k < dsi && __ldg(adj + rb + k) == a.x; ++k)
+                            pu = radd(pu, x);
+                        pvec[a.x] = pu;
+                        pcost += a.y;
+                        mx = std_max(mx, pu);
+                        mn = std_min(mn, pu);
+                    }
+                    const unsigned bl = __ballot_sync(kFullMask, lead);
+                    if (lead) qn[found + __popc(bl & lt)] = a.x;
+                    found += __popc(bl);
+                }
+                __syncwarp();
+                // (2) preds[s -> t] = 1/ds + (pvec[s] - pvec[t]) / ds with the round's residuals
+                const Real ps = pvec[src];
+                for (uint32_t o = lane; o < dsi; o += 32)
+                    p.preds[rb + o] = row_update<Real, Acc>(pinit, ps, pvec[__ldg(adj + rb + o)], ds);
+                qs = found;
+            } else {
             pipelined<uint2>(dsi,
                 [&](uint32_t c, uint2* r) {
     #pragma unroll
@@ -1566,9 +1606,10 @@ source_kernel(SourceParams<Real, Acc> p) {
                         p.preds[rb + o] = row_update<Real, Acc>(pinit, Real(0), pu, ds);
                     }
                 });
+            qs = dsi;
+            }
             st_pv += 1;
             st_tr += dsi;
-            qs = dsi;
             ell = 1;
             { uint32_t* tmp = q; q = qn; qn = tmp; }
             __syncwarp();
@@ -1674,8 +1715,22 @@ source_kernel(SourceParams<Real, Acc> p) {
                                 }
                                 const bool act = c0 + lane < vd;
                                 const uint32_t cu = cur[jj].x, cd = cur[jj].y;
+                                // a run of one repeated neighbour (adjacent lanes: rows are
+                                // sorted) is applied by its first lane, one add per repeat in
+                                // order; runs continued from the previous chunk were applied
+                                // before this one, as the reference's sequential loop does
+                                bool lead = act;
+                                uint32_t reps = 1;
+                                if (!JACOBI && p.multi) {
+                                    const uint32_t pcu = __shfl_up_sync(kFullMask, cu, 1);
+                                    const bool follow = act && lane > 0 && pcu == cu;
+                                    const unsigned fb = __ballot_sync(kFullMask, follow);
+                                    lead = act && !follow;
+                                    const unsigned rest = lane == 31 ? 0u : (fb >> (lane + 1));
+                                    reps = uint32_t(__ffs(int(~rest)));
+                                }
                                 bool fresh = false;
-                                if (act && vis[cu] == 0) {
+                                if (lead && vis[cu] == 0) {
                                     vis[cu] = 1;
                                     fresh = true;
                                 }
@@ -1685,7 +1740,12 @@ source_kernel(SourceParams<Real, Acc> p) {
                                     pcost += cd;
                                 }
                                 qns += __popc(bal);
-                                if (act) pvec[cu] = radd(pvec[cu], rdiv(r, from_u64<Real>(cd)));
+                                if (lead) {
+                                    const Real add = rdiv(r, from_u64<Real>(cd));
+                                    Real pv = pvec[cu];
+                                    for (uint32_t k = 0; k < reps; ++k) pv = radd(pv, add);
+                                    pvec[cu] = pv;
+                                }
                                 __syncwarp();
                             }
                         }
@@ -2276,7 +2336,8 @@ finish_kernel(const Acc* __restrict__ preds, const uint32_t* __restrict__ sym_sr
         const uint32_t o = __ldg(sym_src + q);
         const bool first = q == 0 || __ldg(row_of + q - 1) != s;
         // second level, all at once: both rows' marks, both pre-symmetric scores, and the degree of
-        // s (the reverse slot's neighbour degree; tgtp_run takes no repeated neighbours)
+        // s (the reverse slot's neighbour degree; only graphs without repeated neighbours or
+        // self-loops have rows in closed form, every row of the others is listed)
         const uint32_t r = o ? o - 1 : 0;
         const bool ls = __ldg(mark + s) == epoch;
         const bool lt = o && __ldg(mark + tv.x) == epoch;  // slot r lies in row tv.x
@@ -2359,6 +2420,17 @@ void prepare_split_tables(tgtp_graph* g, uint32_t omega) {
         total, g->wtab64.as<double>(), g->wtab32.as<float>());
     TGTP_LAUNCH_CHECK("split_tables_kernel");
     g->split_omega = omega;
+}
+
+// Graphs with repeated neighbours or self-loops: every row is listed before the tau kernels run
+// (so none is scored in closed form, which assumes distinct neighbours and pvec[s] = 0 after the
+// first round), and the tau kernels, finding every row marked, append none.
+__global__ void list_all_rows_kernel(RowMarks rm, uint32_t n) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        rm.mark[r] = rm.epoch;
+        rm.list[r] = r;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *rm.len = n;
 }
 
 // Row marks of this run: they sit behind the work words in the counter buffer, so the run's one
@@ -2472,6 +2544,14 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     TGTP_CUDA(cudaMemsetAsync(stats, 0, zero_bytes, s));
 
     const RowMarks rm = begin_row_marks(g);
+    const bool multi = !JACOBI && g->has_multi_edges;
+    if (multi) {
+        // the reference leaves tau = 0 in the slots no forward edge writes (the later repeats of
+        // a neighbour u < v in row v, src/aesc.h:179-209), and every row goes to the source kernel
+        TGTP_CUDA(cudaMemsetAsync(g->taus.ptr, 0, sizeof(int) * m, s));
+        list_all_rows_kernel<<<grid_cap(n, 256, g->num_sms, 8), 256, 0, s>>>(rm, uint32_t(n));
+        TGTP_LAUNCH_CHECK("list_all_rows_kernel");
+    }
     if constexpr (JACOBI || std::is_same<Real, double>::value) {
         // FP64 and mixed forms: eight lanes per edge over F64 / F32 / BF16 rows
         prepare_split_tables(g, omega);
@@ -2659,6 +2739,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.pre = nullptr;
     p.pre_cols = nullptr;
     p.pre_final = nullptr;
+    p.multi = multi;
     if (!block_mode) {
         p.claim = work;
         p.list_base = 0;
@@ -2755,8 +2836,10 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
     if (g->min_degree == 0)
         fail(TGTP_ERR_INVALID_ARGUMENT,
              "graph vertex IDs must be contiguous with no isolated vertices");
-    if (g->has_multi_edges)
-        fail(TGTP_ERR_UNSUPPORTED, "rows with repeated neighbours are not supported by tgtp_run");
+    if (g->has_multi_edges && cfg.precision == TGTP_PRECISION_MIXED)
+        fail(TGTP_ERR_UNSUPPORTED,
+             "the mixed form does not take rows with repeated neighbours or self-loops; "
+             "use the FP32 or FP64 form");
     switch (cfg.precision) {
         case TGTP_PRECISION_FP32:
             if (!g->has_f32) fail(TGTP_ERR_INVALID_ARGUMENT, "FP32 form needs F32 eigenvectors");

@@ -186,6 +186,10 @@ struct tgtp_graph {
     // walk copy of the graph renumbered by degree (built on the first saba_count)
     tgtp::DeviceBuffer saba_info, saba_adj, saba_cnt;
     bool saba_ready = false;
+    // the same copy with each slot holding its target's row record (16 bytes per slot; built on
+    // the first saba_count that walks the inlined copy)
+    tgtp::DeviceBuffer saba_adj16;
+    bool saba_inline_ready = false;
     int32_t last_precision = -1;
     bool have_run = false;
 

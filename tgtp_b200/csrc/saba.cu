@@ -253,6 +253,116 @@ saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict
     if (lane == 0 && f) atomicAdd(fallback_total, (unsigned long long)f);
 }
 
+// ---- walk copy with the next row inlined in each slot ------------------------------------------------
+// A hop of saba_walk_perm_kernel makes two dependent random loads: the chosen slot (the next vertex
+// p) and then p's 16-byte row record.  In this copy, slot q of the renumbered adjacency holds the
+// record of the vertex it points to: (row start, degree, fmix32(original id), p).  A hop is then one
+// dependent 16-byte load; the counter update (p) stays off the dependent chain.  The copy takes
+// 16 bytes per slot (4 x the plain renumbered adjacency).
+__global__ void saba_adj16_kernel(const uint32_t* __restrict__ adjp, const uint4* __restrict__ info,
+                                  uint64_t m, uint4* __restrict__ adj16) {
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < m;
+         q += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t p = adjp[q];
+        const uint4 r = info[p];
+        adj16[q] = make_uint4(r.x, r.y, fmix32(r.z), p);
+    }
+}
+
+// The walk over the inlined copy: trajectories, hashes and fallbacks exactly as
+// saba_walk_perm_kernel (the hash of the primary phase is read precomputed from the slot).
+template <int WPL>
+__global__ void __launch_bounds__(kSabaThreads)
+saba_walk_inline_kernel(const uint4* __restrict__ info, const uint4* __restrict__ adj16,
+                        uint32_t depth, uint32_t bouquets_per_src, uint32_t grid_step,
+                        uint64_t total_bouquets, uint32_t* __restrict__ cnt, uint32_t hot,
+                        unsigned long long* __restrict__ fallback_total) {
+    extern __shared__ uint32_t s_cnt[];
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+
+    const uint32_t lane = threadIdx.x & 31, j = lane & 7, grp = lane >> 3;
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    constexpr uint32_t SB = 4 * WPL;  // bouquets per warp step
+    const uint64_t steps = (total_bouquets + SB - 1) / SB;
+    const uint64_t s_lo = steps * warp / nwarps, s_hi = steps * (warp + 1) / nwarps;
+
+    uint32_t src[WPL], bq[WPL];
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) {
+        const uint64_t b = s_lo * SB + uint32_t(w) * 4 + grp;
+        src[w] = uint32_t(b / bouquets_per_src);
+        bq[w] = uint32_t(b - uint64_t(src[w]) * bouquets_per_src);
+    }
+    uint32_t fallbacks = 0;
+    for (uint64_t st = s_lo; st < s_hi; ++st) {
+        bool active[WPL], primary[WPL];
+        uint32_t beg[WPL], d[WPL], hsh[WPL], secret[WPL], state[WPL];
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) {
+            const uint64_t b = st * SB + uint32_t(w) * 4 + grp;
+            active[w] = b < total_bouquets;
+            beg[w] = d[w] = hsh[w] = 0;
+            if (active[w]) {
+                const uint4 r = __ldg(info + src[w]);
+                beg[w] = r.x;
+                d[w] = r.y;
+                hsh[w] = fmix32(r.z);
+                active[w] = r.y != 0;  // isolated sources are skipped (:197-198)
+            }
+            secret[w] = (bq[w] * 8u + j + 1u) * grid_step;
+            state[w] = secret[w];
+            primary[w] = true;
+        }
+        for (uint32_t len = 0; len < depth; ++len) {
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                const unsigned zero =
+                    __ballot_sync(kFullMask, active[w] && primary[w] && secret[w] == 0u);
+                if ((zero >> (grp * 8)) & 0xffu) primary[w] = false;
+            }
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                if (active[w]) {
+                    uint32_t k;
+                    if (primary[w]) {
+                        k = __umulhi(secret[w] ^ hsh[w], d[w]);
+                        secret[w] *= d[w];
+                    } else {
+                        k = splitmix32(state[w]) % d[w];
+                    }
+                    const uint4 e = __ldg(adj16 + beg[w] + k);
+                    beg[w] = e.x;
+                    d[w] = e.y;
+                    hsh[w] = e.z;
+                    if (e.w < hot) atomicAdd(s_cnt + e.w, 1u);
+                    else atomicAdd(cnt + e.w, 1u);
+                }
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) {
+            if (active[w] && !primary[w] && j == 0) ++fallbacks;
+            bq[w] += SB;
+            while (bq[w] >= bouquets_per_src) {
+                bq[w] -= bouquets_per_src;
+                ++src[w];
+            }
+        }
+    }
+
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
+        const uint32_t c = s_cnt[i];
+        if (c) atomicAdd(cnt + i, c);
+    }
+    uint32_t f = fallbacks;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) f += __shfl_xor_sync(kFullMask, f, o);
+    if (lane == 0 && f) atomicAdd(fallback_total, (unsigned long long)f);
+}
+
 // visit_count = sum c[v], checksum = sum (v+1) c[v], both exact in 64 bits.
 __global__ void saba_sums_kernel(const uint32_t* __restrict__ c, uint64_t n,
                                  unsigned long long* __restrict__ out) {
@@ -321,6 +431,28 @@ void saba_prepare(tgtp_graph* g) {
     g->saba_ready = true;
 }
 
+// Whether saba_count walks the inlined copy (one dependent 16-byte load per hop) or the plain
+// renumbered copy (two): TGTP_SABA_INLINE=0/1 decides, else the inlined copy is used while its
+// 16 bytes per slot stay within 2 GiB.
+bool saba_use_inline(const tgtp_graph* g) {
+    if (const char* e = std::getenv("TGTP_SABA_INLINE")) return std::atoi(e) != 0;
+    return g->m * sizeof(uint4) <= (size_t(2) << 30);
+}
+
+void saba_prepare_inline(tgtp_graph* g) {
+    if (g->saba_inline_ready) return;
+    saba_prepare(g);
+    cudaStream_t s = g->stream;
+    g->saba_adj16.reserve(sizeof(uint4) * (g->m + 1));
+    if (g->m) {
+        const unsigned mb = unsigned(std::min<uint64_t>((g->m + 255) / 256, 8u * g->num_sms));
+        saba_adj16_kernel<<<mb, 256, 0, s>>>(g->saba_adj.as<uint32_t>(), g->saba_info.as<uint4>(),
+                                             g->m, g->saba_adj16.as<uint4>());
+        TGTP_LAUNCH_CHECK("saba_adj16_kernel");
+    }
+    g->saba_inline_ready = true;
+}
+
 template <int WPL>
 void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step, uint64_t total,
                  uint32_t* cnt, unsigned long long* fb) {
@@ -330,20 +462,29 @@ void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step
     cap = std::max<uint32_t>(1024u, std::min<uint32_t>(cap, 53248u));
     const uint32_t hot = uint32_t(g->n < cap ? g->n : cap);
     const size_t smem = sizeof(uint32_t) * hot;
-    TGTP_CUDA(cudaFuncSetAttribute(saba_walk_perm_kernel<WPL>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const bool inl = saba_use_inline(g);
+    if (inl) saba_prepare_inline(g);
+    const void* kern = inl ? reinterpret_cast<const void*>(saba_walk_inline_kernel<WPL>)
+                           : reinterpret_cast<const void*>(saba_walk_perm_kernel<WPL>);
+    TGTP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
-    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, saba_walk_perm_kernel<WPL>,
-                                                            kSabaThreads, smem));
+    TGTP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSabaThreads, smem));
     if (per_sm < 1) per_sm = 1;
     uint64_t blocks = uint64_t(g->num_sms) * per_sm;
     const uint64_t need = (total + 4 * WPL - 1) / (4 * WPL) / (kSabaThreads / 32) + 1;
     if (blocks > need) blocks = need;
     ScopedKernel k(g->prof, s, "saba_walk");
-    saba_walk_perm_kernel<WPL><<<unsigned(blocks), kSabaThreads, smem, s>>>(
-        g->saba_info.as<uint4>(), g->saba_adj.as<uint32_t>(), depth, bps, grid_step, total, cnt,
-        hot, fb);
-    TGTP_LAUNCH_CHECK("saba_walk_perm_kernel");
+    if (inl) {
+        saba_walk_inline_kernel<WPL><<<unsigned(blocks), kSabaThreads, smem, s>>>(
+            g->saba_info.as<uint4>(), g->saba_adj16.as<uint4>(), depth, bps, grid_step, total,
+            cnt, hot, fb);
+        TGTP_LAUNCH_CHECK("saba_walk_inline_kernel");
+    } else {
+        saba_walk_perm_kernel<WPL><<<unsigned(blocks), kSabaThreads, smem, s>>>(
+            g->saba_info.as<uint4>(), g->saba_adj.as<uint32_t>(), depth, bps, grid_step, total,
+            cnt, hot, fb);
+        TGTP_LAUNCH_CHECK("saba_walk_perm_kernel");
+    }
 }
 
 void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_counters) {
