@@ -202,6 +202,19 @@ tgtp_status saba_count_static(const uint32_t* device_idx, const uint32_t* device
                               uint32_t depth, uint32_t n_walks, void* cuda_stream,
                               saba_result* out);
 
+/* ---- exact spanning centrality of sampled edges (the accuracy reference) -------------------- */
+/* The quantity of src/exact_sc.cpp:24-49 (and scripts/paper_accuracy.py:13-54) for graphs too large
+ * for its dense solve: R(u, v) = (e_u - e_v)^T L^+ (e_u - e_v) for each listed CSR slot (u, v), on the
+ * simple graph of the CSR (a repeated neighbour counts once, self-loops are ignored; a self-loop slot
+ * gives 0).  Jacobi-preconditioned conjugate gradients in FP64 on the device, 32 slots at a time;
+ * every slot iterates until its residual norm is at most tol * ||e_u - e_v|| (TGTP_ERR_TIMEOUT when
+ * max_iter iterations do not get there).  host_iterations (may be NULL) receives the iteration count
+ * of each batch of 32 slots (ceil(count / 32) entries).  Synchronous; scratch is allocated per call
+ * (5 blocks of n x 32 doubles). */
+tgtp_status tgtp_exact_sc_slots(tgtp_graph* g, const uint32_t* host_slots, uint32_t count,
+                                double tol, uint32_t max_iter, double* host_resistance,
+                                uint32_t* host_iterations);
+
 /* ---- memory ---------------------------------------------------------------------------------- */
 /* Device blocks of released graphs are kept for reuse (creating a graph per input would otherwise
  * pay cudaMalloc/cudaFree for its scratch every time).  This returns every cached block to the

@@ -227,3 +227,14 @@ def saba_count(g: AESCGraph, depth: int, n_walks: int, counters: bool = True):
     check(lib().saba_count(g.handle, depth, n_walks, ptr(out) if out is not None else None,
                            C.byref(res)))
     return out, int(res.visit_count), int(res.checksum), int(res.fallback_bouquets)
+
+
+def exact_sc_slots(g: AESCGraph, slots, tol: float = 1e-10, max_iter: int = 20000):
+    """Exact spanning centrality (effective resistance) of the given CSR slots on the device:
+    (resistances float64[len(slots)], iterations per batch of 32 slots)."""
+    slots = np.ascontiguousarray(slots, dtype=np.uint32)
+    out = np.empty(len(slots), np.float64)
+    iters = np.zeros(max(1, (len(slots) + 31) // 32), np.uint32)
+    check(lib().tgtp_exact_sc_slots(g.handle, ptr(slots), len(slots), tol, max_iter, ptr(out),
+                                    ptr(iters)))
+    return out, iters

@@ -32,7 +32,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I" + INCLUDE, "-I" + CSRC,
              "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["api.cu", "saba.cu", "aesc.cu", "batch.cu"]
+CU_SOURCES = ["api.cu", "saba.cu", "aesc.cu", "batch.cu", "exact_sc.cu"]
 CPP_SOURCES = ["host_io.cpp"]
 RUNNERS = {"tgtp": "tgtp_main.cpp", "benchmark": "benchmark_main.cpp",
            "rw_experiment_saba": "rw_experiment_saba_main.cpp"}

@@ -1148,7 +1148,8 @@ struct PushBlockParams {
     float* cols;           // per CTA: two n x S blocks
     uint32_t* final_buf;   // per CTA: the block that holds the final columns
     PrePush* pre;          // per list entry
-    bool bits;             // the row bitmasks fit in shared memory
+    bool bits;             // the row bitmasks fit in shared memory (else they live in gbits)
+    uint32_t* gbits;       // per CTA: two n-bit row masks in global memory (L2), when not in smem
     unsigned long long* stats;
     uint64_t budget_ns;
 };
@@ -1156,8 +1157,9 @@ struct PushBlockParams {
 __global__ void __launch_bounds__(1024, 1)
 push_block_kernel(PushBlockParams p) {
     constexpr int S = kBlockCols;
-    // With p.bits: one bit per row, set when a running column of the row is nonzero (cur and nxt
-    // rounds); the pull skips the 128-byte reads of neighbour rows whose bit is clear.
+    // One bit per row, set when a running column of the row is nonzero (cur and nxt rounds); the
+    // pull skips the 128-byte reads of neighbour rows whose bit is clear.  The two masks live in
+    // shared memory while they fit (p.bits), else in this CTA's part of p.gbits (L2-resident).
     extern __shared__ uint32_t s_bits[];
     __shared__ uint32_t s_src[S], s_rb[S], s_ds[S], s_support[S], s_ell[S];
     __shared__ unsigned long long s_picost[S];
@@ -1181,10 +1183,10 @@ push_block_kernel(PushBlockParams p) {
     for (size_t i = threadIdx.x; i < size_t(n) * S / 4; i += blockDim.x)
         reinterpret_cast<float4*>(A)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t words = (n + 31) / 32;
-    uint32_t* bcur = s_bits;
-    uint32_t* bnxt = s_bits + words;
-    if (p.bits)
-        for (uint32_t i = threadIdx.x; i < 2 * words; i += blockDim.x) s_bits[i] = 0u;
+    uint32_t* const bits_base = p.bits ? s_bits : p.gbits + size_t(blockIdx.x) * 2 * words;
+    uint32_t* bcur = bits_base;
+    uint32_t* bnxt = bits_base + words;
+    for (uint32_t i = threadIdx.x; i < 2 * words; i += blockDim.x) bits_base[i] = 0u;
     if (threadIdx.x < S) {
         const uint32_t j = threadIdx.x;
         s_active[j] = j < cnt;
@@ -1206,7 +1208,7 @@ push_block_kernel(PushBlockParams p) {
             const uint2 a = __ldg(p.adjd + rb + o);
             const float pu = from_fixed(kFixOne, a.y);
             A[size_t(a.x) * S + j] = pu;
-            if (p.bits) atomicOr(bcur + (a.x >> 5), 1u << (a.x & 31));
+            atomicOr(bcur + (a.x >> 5), 1u << (a.x & 31));
             pc += a.y;
             mx = fmaxf(mx, pu);
             mn = fminf(mn, pu);
@@ -1289,8 +1291,7 @@ push_block_kernel(PushBlockParams p) {
             s_min[threadIdx.x] = __float_as_uint(1.f);
             s_support[threadIdx.x] = 0;
         }
-        if (p.bits)
-            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
         __syncthreads();
         const bool run = lane < cnt && s_active[lane];
         unsigned long long pc = 0;
@@ -1306,7 +1307,7 @@ push_block_kernel(PushBlockParams p) {
                 // fixed-point sum does not depend on the order)
                 const bool in = c + lane < ud;
                 const unsigned live = __ballot_sync(
-                    kFullMask, in && (!p.bits || ((bcur[nb >> 5] >> (nb & 31)) & 1u)));
+                    kFullMask, in && ((bcur[nb >> 5] >> (nb & 31)) & 1u));
                 const uint32_t nth = lane < uint32_t(__popc(live)) ? __fns(live, 0, int(lane) + 1) : 0u;
                 const uint32_t packed = __shfl_sync(kFullMask, nb, nth);
                 const uint32_t k = __popc(live);
@@ -1331,7 +1332,7 @@ push_block_kernel(PushBlockParams p) {
                     mn = fminf(mn, r);
                 }
             }
-            if (p.bits && __any_sync(kFullMask, run && r > 0.f) && lane == 0)
+            if (__any_sync(kFullMask, run && r > 0.f) && lane == 0)
                 atomicOr(bnxt + (u >> 5), 1u << (u & 31));
             nxt[size_t(u) * S + lane] = r;
         }
@@ -1362,6 +1363,30 @@ push_block_kernel(PushBlockParams p) {
         bcur = bnxt;
         bnxt = tb;
         fin ^= 1u;
+    }
+    // The final columns, transposed into the other buffer: column j becomes n contiguous floats
+    // at spare + j * n, so the per-source stage reads its residual vector with unit stride.  Warp
+    // w takes tiles of 32 rows; lane l loads row (tile + l) whole (eight 16-byte loads of one
+    // 128-byte row) and the 32 stores of the tile (one per column) are each 128 contiguous bytes.
+    {
+        float* spare = fin ? A : B;
+        for (uint32_t t0 = warp * 32u; t0 < n; t0 += nwarp * 32u) {
+            const uint32_t u = t0 + lane;
+            float v[S];
+            if (u < n) {
+                const float4* row = reinterpret_cast<const float4*>(cur + size_t(u) * S);
+#pragma unroll
+                for (int k = 0; k < S / 4; ++k) {
+                    const float4 f = row[k];
+                    v[4 * k] = f.x;
+                    v[4 * k + 1] = f.y;
+                    v[4 * k + 2] = f.z;
+                    v[4 * k + 3] = f.w;
+                }
+#pragma unroll
+                for (int c = 0; c < S; ++c) spare[size_t(c) * n + u] = v[c];
+            }
+        }
     }
     if (threadIdx.x == 0) p.final_buf[blockIdx.x] = fin;
     st_pv = warp_sum_u64(st_pv);
@@ -1518,18 +1543,22 @@ source_kernel(SourceParams<Real, Acc> p) {
         };
         lap(0);
         if (p.pre) {
-            // The push ran in push_block_kernel: take the source's final residual vector from its
-            // column and rebuild the final frontier (the support) in vertex order.
+            // The push ran in push_block_kernel, which left the source's final residual vector as
+            // n contiguous floats (its column, transposed into the CTA's other block buffer).  The
+            // HBM tier reads it in place; the shared-memory tier copies it.  The final frontier
+            // (the support) is rebuilt in vertex order.
             const PrePush pr = p.pre[entry];
             const uint32_t slot = entry - p.list_base;
             const uint32_t cta = slot / kBlockCols, col = slot % kBlockCols;
             const float* cb = p.pre_cols +
-                              (size_t(cta) * 2 + p.pre_final[cta]) * size_t(n) * kBlockCols + col;
+                              (size_t(cta) * 2 + (1u - p.pre_final[cta])) * size_t(n) * kBlockCols +
+                              size_t(col) * n;
+            if constexpr (!SMEM && std::is_same<Real, float>::value) pvec = const_cast<Real*>(cb);
             uint32_t cq = 0;
             for (uint32_t i0 = 0; i0 < n; i0 += 32) {
                 const uint32_t i = i0 + lane;
-                const Real x = i < n ? Real(cb[size_t(i) * kBlockCols]) : Real(0);
-                if (i < n) pvec[i] = x;
+                const Real x = i < n ? Real(cb[i]) : Real(0);
+                if (SMEM && i < n) pvec[i] = x;
                 const bool nz = x > Real(0);
                 const unsigned bal = __ballot_sync(kFullMask, nz);
                 if (nz) q[cq + __popc(bal & lt)] = i;
@@ -2267,6 +2296,13 @@ source_kernel(SourceParams<Real, Acc> p) {
         lap(6);
         // ---- next source starts from an all-zero residual vector ----
         __syncwarp();
+        if (!SMEM && p.pre) {
+            // the residual vector was the block push's column, read in place: the warp's own
+            // vector is untouched (and the flags used by the edge bound are back to zero)
+            pvec = p.pvec_g + gw * size_t(n);
+            lap(7);
+            continue;
+        }
         pipelined<uint32_t>(qs,
             [&](uint32_t i0, uint32_t* r) {
 #pragma unroll
@@ -2524,12 +2560,15 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
     else block_mode = JACOBI && g->push_hint[key] == 2;
     g->last_key = key;
-    // CTAs of the block push: one per SM, within a 24 GB budget for their residual blocks
+    // CTAs of the block push: one per SM, within a budget for their residual blocks of 24 GB or
+    // half the device memory free now (beside what the blocks already hold), whichever is larger
     // (TGTP_BLOCK_CTAS lowers the count, e.g. to exercise many waves on small graphs)
     uint32_t block_ctas = uint32_t(g->num_sms);
-    {
+    if (block_mode) {
         const size_t per_cta = 2 * size_t(n) * kBlockCols * sizeof(float);
-        const size_t budget = size_t(24) << 30;
+        size_t free_b = 0, total_b = 0;
+        TGTP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t budget = std::max(size_t(24) << 30, (free_b + g->block_cols.bytes) / 2);
         block_ctas = uint32_t(std::max<size_t>(1, std::min<size_t>(block_ctas, budget / per_cta)));
         if (const char* e = std::getenv("TGTP_BLOCK_CTAS"))
             block_ctas = std::max(1u, std::min(block_ctas, uint32_t(std::atoi(e))));
@@ -2772,6 +2811,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         const size_t bits_bytes = 2 * sizeof(uint32_t) * ((size_t(n) + 31) / 32);
         bp.bits = bits_bytes <= size_t(200) * 1024;
         const size_t bsm = bp.bits ? bits_bytes : 0;
+        if (!bp.bits) grow(g, g->block_bits, bits_bytes * block_ctas + 16);
+        bp.gbits = bp.bits ? nullptr : g->block_bits.as<uint32_t>();
         if (bsm) (void)blocks_per_sm(reinterpret_cast<const void*>(push_block_kernel), 1024, bsm);
         p.pre = bp.pre;
         p.pre_cols = bp.cols;
