@@ -1139,6 +1139,7 @@ struct PushBlockParams {
     const uint32_t* deg;
     const uint2* adjd;
     uint32_t n;
+    uint64_t m;
     const int* taus;
     double* preds;
     unsigned* work;        // [1] error flags, [2] list length
@@ -1148,24 +1149,89 @@ struct PushBlockParams {
     float* cols;           // per CTA: two n x S blocks
     uint32_t* final_buf;   // per CTA: the block that holds the final columns
     PrePush* pre;          // per list entry
-    bool bits;             // the row bitmasks fit in shared memory (else they live in gbits)
-    uint32_t* gbits;       // per CTA: two n-bit row masks in global memory (L2), when not in smem
+    bool bits;             // the three row masks fit in shared memory (else they live in gbits)
+    uint32_t* gbits;       // per CTA: three n-bit row masks in global memory (L2), when not in smem
+    uint32_t* lists;       // per CTA: four row lists of n entries (see push_block_kernel)
+    uint32_t list_div;     // a round is compacted when its live rows' degree sum * list_div < m
+    int rounds_mode;       // 0 = by that rule, 1 = every round compacted, 2 = every round full
     unsigned long long* stats;
     uint64_t budget_ns;
 };
 
+// Exclusive prefix sum over the block's threads (blockDim.x a multiple of 32, at most 1024); the
+// block total goes to *total.  Uses `tmp` (32 words of shared memory).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* tmp, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= uint32_t(o)) incl += y;
+    }
+    if (lane == 31) tmp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < nwarp ? tmp[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFullMask, wi, o);
+            if (lane >= uint32_t(o)) wi += y;
+        }
+        if (lane < nwarp) tmp[lane] = wi - w;
+        if (lane == 31) *total = wi;
+    }
+    __syncthreads();
+    const uint32_t out = tmp[warp] + incl - v;
+    __syncthreads();
+    return out;
+}
+
+// The rows whose bit is set in `mask` (words of 32 rows), in increasing order, into `out`; the
+// count goes to *count.  Each thread takes a contiguous run of words.
+__device__ __forceinline__ void compact_mask(const uint32_t* mask, uint32_t words, uint32_t n,
+                                             uint32_t* out, uint32_t* tmp, uint32_t* count) {
+    const uint32_t per = (words + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = min(words, threadIdx.x * per), w1 = min(words, w0 + per);
+    uint32_t c = 0;
+    for (uint32_t w = w0; w < w1; ++w) c += __popc(mask[w]);
+    uint32_t pos = block_exclusive_scan(c, tmp, count);
+    for (uint32_t w = w0; w < w1; ++w) {
+        uint32_t b = mask[w];
+        while (b) {
+            const uint32_t r = w * 32u + uint32_t(__ffs(b) - 1);
+            b &= b - 1;
+            if (r < n) out[pos++] = r;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(1024, 1)
 push_block_kernel(PushBlockParams p) {
     constexpr int S = kBlockCols;
-    // One bit per row, set when a running column of the row is nonzero (cur and nxt rounds); the
-    // pull skips the 128-byte reads of neighbour rows whose bit is clear.  The two masks live in
-    // shared memory while they fit (p.bits), else in this CTA's part of p.gbits (L2-resident).
+    // Row masks, one bit per row: bcur / bnxt mark the rows with a nonzero running column in the
+    // cur / nxt block (the pull skips the 128-byte reads of neighbour rows whose bit is clear);
+    // tmask marks the rows a compacted round processes.  In shared memory while the three fit
+    // (p.bits), else in this CTA's part of p.gbits (L2-resident).
+    //
+    // Row lists (n entries each, in p.lists): Lc = rows with any nonzero column in cur, Lp = the
+    // same for the block nxt still holds from the round before, Ln = those of the round being
+    // formed, P = the rows a compacted round processes.  A round is either a full pass over all n
+    // rows (dense frontiers) or a compacted one over P = (neighbours of the running-live rows of
+    // cur) U Lc U Lp, in increasing row order: a row outside the neighbourhood of the live rows
+    // receives nothing, Lc carries the stopped columns and zeroes the running ones, and Lp covers
+    // every row nxt still holds from two rounds before, so no stale row survives.  Both give the
+    // same values; the choice per round is by the live rows' degree sum (the scatter work of the
+    // compaction) against m / list_div.
     extern __shared__ uint32_t s_bits[];
     __shared__ uint32_t s_src[S], s_rb[S], s_ds[S], s_support[S], s_ell[S];
     __shared__ unsigned long long s_picost[S];
     __shared__ unsigned s_max[S], s_min[S];  // float bits of non-negative residuals
     __shared__ int s_active[S];
     __shared__ int s_any;
+    __shared__ uint32_t s_tmp[32];
+    __shared__ uint32_t s_lc, s_lp, s_ln, s_pn;  // list lengths
+    __shared__ unsigned long long s_live_deg;   // degree sum of the running-live rows of cur
     pdl_launch_dependents();
     pdl_wait();  // the list, and the previous wave's readers of these blocks
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -1179,14 +1245,20 @@ push_block_kernel(PushBlockParams p) {
     const uint64_t deadline = globaltimer_ns() + p.budget_ns;
     unsigned long long st_pv = 0, st_tr = 0, st_rounds = 0;
 
-    // round 1 in closed form: the frontier {src} pushes 1 / deg(u) to every neighbour u
-    for (size_t i = threadIdx.x; i < size_t(n) * S / 4; i += blockDim.x)
+    // both blocks start at zero (a compacted round writes only the rows it processes)
+    for (size_t i = threadIdx.x; i < size_t(n) * S / 2; i += blockDim.x)
         reinterpret_cast<float4*>(A)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t words = (n + 31) / 32;
-    uint32_t* const bits_base = p.bits ? s_bits : p.gbits + size_t(blockIdx.x) * 2 * words;
+    uint32_t* const bits_base = p.bits ? s_bits : p.gbits + size_t(blockIdx.x) * 3 * words;
     uint32_t* bcur = bits_base;
     uint32_t* bnxt = bits_base + words;
-    for (uint32_t i = threadIdx.x; i < 2 * words; i += blockDim.x) bits_base[i] = 0u;
+    uint32_t* tmask = bits_base + 2 * words;
+    for (uint32_t i = threadIdx.x; i < 3 * words; i += blockDim.x) bits_base[i] = 0u;
+    uint32_t* const lbase = p.lists + size_t(blockIdx.x) * 4 * size_t(n);
+    uint32_t* Lc = lbase;
+    uint32_t* Lp = lbase + n;
+    uint32_t* Ln = lbase + 2 * size_t(n);
+    uint32_t* const P = lbase + 3 * size_t(n);
     if (threadIdx.x < S) {
         const uint32_t j = threadIdx.x;
         s_active[j] = j < cnt;
@@ -1196,7 +1268,12 @@ push_block_kernel(PushBlockParams p) {
         s_min[j] = __float_as_uint(1.f);
         s_ell[j] = 1;
     }
+    if (threadIdx.x == 0) {
+        s_lp = 0;
+        s_live_deg = 0;
+    }
     __syncthreads();
+    // round 1 in closed form: the frontier {src} pushes 1 / deg(u) to every neighbour u
     if (warp < cnt) {
         const uint32_t j = warp, src = s_src[j];
         const uint32_t rb = __ldg(p.idx + src), dsi = __ldg(p.idx + src + 1) - rb;
@@ -1227,6 +1304,16 @@ push_block_kernel(PushBlockParams p) {
         }
         st_pv += lane == 0 ? 1 : 0;
         st_tr += lane == 0 ? dsi : 0;
+    }
+    __syncthreads();
+    // Lc after round 1: the rows of bcur (every column runs, so a nonzero row is running-live)
+    compact_mask(bcur, words, n, Lc, s_tmp, &s_lc);
+    __syncthreads();
+    {
+        unsigned long long d = 0;
+        for (uint32_t k = threadIdx.x; k < s_lc; k += blockDim.x) d += __ldg(p.deg + Lc[k]);
+        d = warp_sum_u64(d);
+        if (lane == 0 && d) atomicAdd(&s_live_deg, d);
     }
     __syncthreads();
     float* cur = A;
@@ -1284,6 +1371,29 @@ push_block_kernel(PushBlockParams p) {
         }
         __syncthreads();
         if (!s_any) break;
+        // ---- the rows this round processes: all n, or the compacted list P ----
+        const bool compact = p.rounds_mode == 1 ||
+                             (p.rounds_mode == 0 &&
+                              double(s_live_deg) * double(p.list_div) < double(p.m));
+        __syncthreads();  // every thread has read s_live_deg before it is reset below
+        if (compact) {
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) tmask[i] = 0u;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < s_lp; k += blockDim.x)
+                atomicOr(tmask + (Lp[k] >> 5), 1u << (Lp[k] & 31));
+            for (uint32_t k = warp; k < s_lc; k += nwarp) {
+                const uint32_t w = Lc[k];
+                if (lane == 0) atomicOr(tmask + (w >> 5), 1u << (w & 31));
+                if (!((bcur[w >> 5] >> (w & 31)) & 1u)) continue;  // only stopped columns here
+                const uint32_t wb = __ldg(p.idx + w), we = __ldg(p.idx + w + 1);
+                for (uint32_t o = wb + lane; o < we; o += 32) {
+                    const uint32_t u = __ldg(p.adj + o);
+                    atomicOr(tmask + (u >> 5), 1u << (u & 31));
+                }
+            }
+            __syncthreads();
+            compact_mask(tmask, words, n, P, s_tmp, &s_pn);
+        }
         // ---- one Jacobi round for the running columns; stopped columns are carried over ----
         if (threadIdx.x < S) {
             s_picost[threadIdx.x] = 0;
@@ -1291,35 +1401,42 @@ push_block_kernel(PushBlockParams p) {
             s_min[threadIdx.x] = __float_as_uint(1.f);
             s_support[threadIdx.x] = 0;
         }
+        if (threadIdx.x == 0) {
+            s_ln = 0;
+            s_live_deg = 0;
+        }
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
         __syncthreads();
+        const uint32_t nrows = compact ? s_pn : n;
         const bool run = lane < cnt && s_active[lane];
-        unsigned long long pc = 0;
+        unsigned long long pc = 0, live_deg = 0;
         uint32_t sup = 0;
         float mx = 0.f, mn = 1.f;
-        for (uint32_t u = warp; u < n; u += nwarp) {
+        for (uint32_t k = warp; k < nrows; k += nwarp) {
+            const uint32_t u = compact ? P[k] : k;
             const uint32_t ub = __ldg(p.idx + u), ud = __ldg(p.idx + u + 1) - ub;
             unsigned long long acc = 0;
             for (uint32_t c = 0; c < ud; c += 32) {
                 const uint32_t nb = c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u;
-                // neighbours whose running columns are all zero add nothing: with the bitmask they
-                // are dropped, and the live ones compacted into lanes 0 .. popc(live) - 1 (the
-                // fixed-point sum does not depend on the order)
+                // neighbours whose running columns are all zero add nothing: they are dropped, and
+                // the live ones compacted into lanes 0 .. popc(live) - 1 (the fixed-point sum does
+                // not depend on the order)
                 const bool in = c + lane < ud;
-                const unsigned live = __ballot_sync(
-                    kFullMask, in && ((bcur[nb >> 5] >> (nb & 31)) & 1u));
-                const uint32_t nth = lane < uint32_t(__popc(live)) ? __fns(live, 0, int(lane) + 1) : 0u;
+                const unsigned live =
+                    __ballot_sync(kFullMask, in && ((bcur[nb >> 5] >> (nb & 31)) & 1u));
+                const uint32_t nth =
+                    lane < uint32_t(__popc(live)) ? __fns(live, 0, int(lane) + 1) : 0u;
                 const uint32_t packed = __shfl_sync(kFullMask, nb, nth);
-                const uint32_t k = __popc(live);
+                const uint32_t kk = __popc(live);
                 uint32_t t = 0;
-                for (; t + 4 <= k; t += 4) {
+                for (; t + 4 <= kk; t += 4) {
                     const float x0 = cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane];
                     const float x1 = cur[size_t(__shfl_sync(kFullMask, packed, t + 1)) * S + lane];
                     const float x2 = cur[size_t(__shfl_sync(kFullMask, packed, t + 2)) * S + lane];
                     const float x3 = cur[size_t(__shfl_sync(kFullMask, packed, t + 3)) * S + lane];
                     acc += to_fixed(x0) + to_fixed(x1) + to_fixed(x2) + to_fixed(x3);
                 }
-                for (; t < k; ++t)
+                for (; t < kk; ++t)
                     acc += to_fixed(cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane]);
             }
             float r = cur[size_t(u) * S + lane];
@@ -1332,8 +1449,15 @@ push_block_kernel(PushBlockParams p) {
                     mn = fminf(mn, r);
                 }
             }
-            if (__any_sync(kFullMask, run && r > 0.f) && lane == 0)
-                atomicOr(bnxt + (u >> 5), 1u << (u & 31));
+            const bool running_live = __any_sync(kFullMask, run && r > 0.f);
+            const bool any_nz = __any_sync(kFullMask, r != 0.f);
+            if (lane == 0) {
+                if (running_live) {
+                    atomicOr(bnxt + (u >> 5), 1u << (u & 31));
+                    live_deg += ud;
+                }
+                if (any_nz) Ln[atomicAdd(&s_ln, 1u)] = u;
+            }
             nxt[size_t(u) * S + lane] = r;
         }
         if (run) {
@@ -1342,6 +1466,7 @@ push_block_kernel(PushBlockParams p) {
             atomicMax(s_max + lane, __float_as_uint(mx));
             atomicMin(s_min + lane, __float_as_uint(mn));
         }
+        if (lane == 0 && live_deg) atomicAdd(&s_live_deg, live_deg);
         __syncthreads();
         // ---- preds[row] += (r[src] - r[t]) / ds for every slot of each running source ----
         if (warp < cnt && s_active[warp]) {
@@ -1355,6 +1480,10 @@ push_block_kernel(PushBlockParams p) {
             }
             if (lane == 0) ++s_ell[j];
         }
+        if (threadIdx.x == 0) {
+            s_lp = s_lc;
+            s_lc = s_ln;
+        }
         __syncthreads();
         float* t = cur;
         cur = nxt;
@@ -1362,6 +1491,10 @@ push_block_kernel(PushBlockParams p) {
         uint32_t* tb = bcur;
         bcur = bnxt;
         bnxt = tb;
+        uint32_t* tl = Lp;
+        Lp = Lc;
+        Lc = Ln;
+        Ln = tl;
         fin ^= 1u;
     }
     // The final columns, transposed into the other buffer: column j becomes n contiguous floats
@@ -2808,11 +2941,28 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         bp.stats = stats;
         bp.budget_ns = p.budget_ns;
         // two row bitmasks in shared memory while they fit beside the kernel's static 1.3 KB
-        const size_t bits_bytes = 2 * sizeof(uint32_t) * ((size_t(n) + 31) / 32);
+        // three row masks in shared memory while they fit beside the kernel's static 1.5 KB,
+        // else in global memory; four row lists of n entries per CTA
+        const size_t bits_bytes = 3 * sizeof(uint32_t) * ((size_t(n) + 31) / 32);
         bp.bits = bits_bytes <= size_t(200) * 1024;
+        if (const char* e = std::getenv("TGTP_BLOCK_MASKS"))  // "global": as for large graphs
+            if (std::string(e) == "global") bp.bits = false;
         const size_t bsm = bp.bits ? bits_bytes : 0;
         if (!bp.bits) grow(g, g->block_bits, bits_bytes * block_ctas + 16);
         bp.gbits = bp.bits ? nullptr : g->block_bits.as<uint32_t>();
+        grow(g, g->block_lists, sizeof(uint32_t) * 4 * size_t(n) * block_ctas + 16);
+        bp.lists = g->block_lists.as<uint32_t>();
+        bp.m = m;
+        // a round is compacted when its live rows' degree sum is below m / list_div
+        // (TGTP_BLOCK_LIST_DIV); TGTP_BLOCK_ROUNDS=compact|full fixes the choice (the values do
+        // not depend on it)
+        bp.list_div = 4;
+        if (const char* e = std::getenv("TGTP_BLOCK_LIST_DIV")) bp.list_div = uint32_t(std::atoi(e));
+        bp.rounds_mode = 0;
+        if (const char* e = std::getenv("TGTP_BLOCK_ROUNDS")) {
+            if (std::string(e) == "compact") bp.rounds_mode = 1;
+            else if (std::string(e) == "full") bp.rounds_mode = 2;
+        }
         if (bsm) (void)blocks_per_sm(reinterpret_cast<const void*>(push_block_kernel), 1024, bsm);
         p.pre = bp.pre;
         p.pre_cols = bp.cols;

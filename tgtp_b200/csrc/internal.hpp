@@ -183,7 +183,8 @@ struct tgtp_graph {
     tgtp::DeviceBuffer taus, preds, stats, counters, sums, scratch, out;
     tgtp::DeviceBuffer tau_sums;  // per forward edge: (upsilon, delta_0) sums of the split forms
     tgtp::DeviceBuffer block_cols, block_pre, block_final, block_keys, block_tmp;  // multi-source push
-    tgtp::DeviceBuffer block_bits;  // the block push's row masks when they do not fit in smem
+    tgtp::DeviceBuffer block_bits;   // the block push's row masks when they do not fit in smem
+    tgtp::DeviceBuffer block_lists;  // the block push's row lists (four of n entries per CTA)
     // walk copy of the graph renumbered by degree (built on the first saba_count)
     tgtp::DeviceBuffer saba_info, saba_adj, saba_cnt;
     bool saba_ready = false;
