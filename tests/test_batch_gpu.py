@@ -122,3 +122,50 @@ def test_batched_graph_keeps_its_buffers(manifest, cuda_device):
     g.upload_eigens(c["values"], c["v32"], VEC_F32)
     assert AESC(g, cfgs[1]).tgtp().shape == (g.m,)
     g.free()
+
+
+@pytest.mark.parametrize("tier", ["smem", "global"])
+@pytest.mark.parametrize("form", ["fp32", "fp64", "mixed_bf16"])
+def test_one_persistent_launch_over_all_graphs_matches_single_runs(manifest, cuda_device, tier,
+                                                                   form, monkeypatch):
+    """Every graph of the batch in one form: their listed rows form one queue that a single
+    persistent source kernel works through (per residual-vector tier), and every graph's scores
+    and work counters equal its single run, on two replays; with the shared kernel switched off
+    (TGTP_BATCH_PERSISTENT=0, one branch per graph) the replays give the same bits too."""
+    import torch
+
+    from tgtp_b200.aesc import (AESC, AESCConfig, Batch, PRECISION_FP32, PRECISION_FP64,
+                                PRECISION_MIXED, VEC_BF16)
+
+    monkeypatch.setenv("TGTP_PVEC_TIER", tier)
+    names = CASES + (["multi300"] if form != "mixed_bf16" else [])
+    prec = {"fp32": PRECISION_FP32, "fp64": PRECISION_FP64, "mixed_bf16": PRECISION_MIXED}[form]
+    graphs, runs, want, stats = [], [], [], []
+    for name in names:
+        c = golden_tgtp_case(manifest, name)
+        g = _graph(c)
+        run = c["runs"][-1]
+        a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"],
+                               precision=prec, vec_dtype=VEC_BF16))
+        want.append(a.tgtp())
+        stats.append(a.stats())
+        graphs.append(g)
+        runs.append((a, torch.empty(g.m, dtype=torch.float32, device="cuda")))
+    for persistent in ("1", "0"):
+        monkeypatch.setenv("TGTP_BATCH_PERSISTENT", persistent)
+        b = Batch([(a, o.data_ptr()) for a, o in runs])
+        for rep in range(2):
+            for _, o in runs:
+                o.fill_(-1.0)
+            b.run()
+            b.wait()
+            for (a, o), w, st in zip(runs, want, stats):
+                got = o.cpu().numpy()
+                assert np.array_equal(got.view(np.uint32), w.view(np.uint32)), (persistent, rep)
+                got_st = a.stats()
+                for k in ("push_rounds", "push_vertices", "push_traversals", "walk_edges",
+                          "walk_count", "walk_hops", "fallback_bouquets"):
+                    assert got_st[k] == st[k], (k, persistent, rep)
+        b.free()
+    for g in graphs:
+        g.free()

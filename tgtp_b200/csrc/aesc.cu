@@ -35,6 +35,8 @@
 #include <cstring>
 #include <string>
 #include <map>
+#include <memory>
+#include <vector>
 #include <mutex>
 #include <tuple>
 #include <type_traits>
@@ -955,7 +957,23 @@ struct SourceParams {
     // keeps duplicate edges and self-loops, src/graph.h:63-66, 75-78): the first round takes the
     // general path and the push serialises each run of a repeated neighbour (parity forms only).
     bool multi;
+    // Vertex count the per-warp scratch is laid out for (the graph's n, or the largest n of a
+    // batch whose graphs share the scratch of one persistent launch).
+    uint32_t scratch_n;
 };
+
+// The source kernel's parameters: one graph (N = 1), or up to N graphs whose listed rows one
+// persistent launch works through as a single queue of (graph, row) items.  Every entry shares the
+// first entry's per-warp scratch (qbuf, items, residual vectors, flags, claim counter).  The pack
+// travels in the kernel's parameter space, so a warp reads its graph's fields from the constant
+// bank with a warp-uniform index.
+template <class Real, class Acc, int N>
+struct SourcePack {
+    static constexpr int kMax = N;
+    uint32_t count;
+    SourceParams<Real, Acc> g[N];
+};
+constexpr int kBatchPack = 64;  // graphs per persistent batch launch
 
 template <class Real>
 __device__ __forceinline__ Real warp_max(Real x) {
@@ -1556,15 +1574,18 @@ __global__ void row_key_kernel(const uint32_t* __restrict__ idx, const int* __re
     }
 }
 
-template <class Real, class Acc, bool SMEM, bool JACOBI>
+template <class Real, class Acc, bool SMEM, bool JACOBI, class Pack>
 __global__ void __launch_bounds__(kSrcMaxThreads)
-source_kernel(SourceParams<Real, Acc> p) {
+source_kernel(Pack pk) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_pre[Pack::kMax + 1];  // item prefix over the pack's row lists
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wib = threadIdx.x >> 5;
     const uint32_t wpb = blockDim.x >> 5;
     const uint64_t gw = uint64_t(blockIdx.x) * wpb + wib;
-    const uint32_t n = p.n;
+    // the per-warp scratch (shared by every graph of the pack) comes from the first entry
+    const SourceParams<Real, Acc>& p0 = pk.g[0];
+    const uint32_t sn = p0.scratch_n;
     const unsigned lt = (1u << lane) - 1u;
     constexpr uint32_t NONE = 0xffffffffu;
     Real* pvec;
@@ -1572,37 +1593,34 @@ source_kernel(SourceParams<Real, Acc> p) {
     unsigned long long* acc;  // 64 per warp: per-slot neighbourhood max (0..31) / min (32..63)
     unsigned long long* fx;   // Jacobi push: per-vertex fixed-point accumulators (all zero between rounds)
     if (SMEM) {
-        unsigned char* base = smem + size_t(wib) * p.smem_per_warp;
+        unsigned char* base = smem + size_t(wib) * p0.smem_per_warp;
         pvec = reinterpret_cast<Real*>(base);
-        const size_t pv = (size_t(n) * sizeof(Real) + 15) & ~size_t(15);
+        const size_t pv = (size_t(sn) * sizeof(Real) + 15) & ~size_t(15);
         vis = base + pv;
-        const size_t vb = (size_t(n) + 15) & ~size_t(15);
+        const size_t vb = (size_t(sn) + 15) & ~size_t(15);
         // the fixed-point accumulators live in shared memory when they fit beside the residual
-        // vector, else in HBM (p.fx_g)
-        const bool fx_here = JACOBI && p.fx_g == nullptr;
+        // vector, else in HBM (p0.fx_g)
+        const bool fx_here = JACOBI && p0.fx_g == nullptr;
         fx = fx_here ? reinterpret_cast<unsigned long long*>(base + pv + vb)
-                     : (JACOBI ? p.fx_g + gw * size_t(n) : nullptr);
+                     : (JACOBI ? p0.fx_g + gw * size_t(sn) : nullptr);
         acc = reinterpret_cast<unsigned long long*>(base + pv + vb +
-                                                    (fx_here ? sizeof(unsigned long long) * n : 0));
+                                                    (fx_here ? sizeof(unsigned long long) * sn : 0));
     } else {
-        pvec = p.pvec_g + gw * size_t(n);
-        vis = p.vis_g + gw * p.vis_stride;
-        fx = JACOBI ? p.fx_g + gw * size_t(n) : nullptr;
+        pvec = p0.pvec_g + gw * size_t(sn);
+        vis = p0.vis_g + gw * p0.vis_stride;
+        fx = JACOBI ? p0.fx_g + gw * size_t(sn) : nullptr;
         acc = reinterpret_cast<unsigned long long*>(smem + size_t(wib) * kAccBytes);
     }
     // pvec and flags are zeroed once, before the warp's first source, unless the warp's last run
     // (same layout, HBM tier) left them zero: every source resets what it touched
-    bool cleared = !SMEM && p.wclean[gw] != 0;
+    bool cleared = !SMEM && p0.wclean[gw] != 0;
     bool dirty = false;  // a source stopped midway (time-out): its vectors are not zero
-    uint32_t* qa = p.qbuf + gw * 2 * size_t(n);
-    uint32_t* qb = qa + n;
-    WalkItem* items = p.items + gw * size_t(p.max_degree);
-    const uint32_t* __restrict__ idx = p.idx;
-    const uint32_t* __restrict__ adj = p.adj;
-    const int* __restrict__ taus = p.taus;
+    uint32_t* qa = p0.qbuf + gw * 2 * size_t(sn);
+    uint32_t* qb = qa + sn;
+    WalkItem* items = p0.items + gw * size_t(p0.max_degree);
     unsigned long long st_rounds = 0, st_pv = 0, st_tr = 0, st_we = 0, st_wc = 0, st_wh = 0,
                        st_fb = 0;
-    const uint64_t deadline = globaltimer_ns() + p.budget_ns;
+    const uint64_t deadline = globaltimer_ns() + p0.budget_ns;
     // SM cycles spent per phase of a source (claim/init, push, post-push, cost test, edge bound,
     // chi/nr, walks, reset), summed over the warp's sources
     long long ph[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1612,33 +1630,91 @@ source_kernel(SourceParams<Real, Acc> p) {
         ph[i] += now - tmark;
         tmark = now;
     };
+
+    // Run counters go to the stats of the graph a source belongs to: flushed when a warp moves
+    // to another graph of the pack, and at the end.
+    auto flush_stats = [&](unsigned long long* stats) {
+        if (lane == 0) {
+            stat_add(stats, kStPushRounds, st_rounds);
+            stat_add(stats, kStPushVertices, st_pv);
+            stat_add(stats, kStPushTraversals, st_tr);
+        }
+        st_we = warp_sum_u64(st_we);
+        st_wc = warp_sum_u64(st_wc);
+        st_wh = warp_sum_u64(st_wh);
+        st_fb = warp_sum_u64(st_fb);
+        if (lane == 0) {
+            stat_add(stats, kStWalkEdges, st_we);
+            stat_add(stats, kStWalkCount, st_wc);
+            stat_add(stats, kStWalkHops, st_wh);
+            stat_add(stats, kStFallback, st_fb);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) stat_add(stats, kStPhase0 + i, (unsigned long long)ph[i]);
+        }
+        st_rounds = st_pv = st_tr = st_we = st_wc = st_wh = st_fb = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) ph[i] = 0;
+    };
     __syncwarp();
 
     pdl_launch_dependents();
-    pdl_wait();  // taus, row list and its length from the tau kernels
-    const unsigned total = p.work[2];  // final: the tau kernel that appends to the list has ended
-    const unsigned nrows = total > p.list_base ? min(total - p.list_base, p.list_cap) : 0u;
-    // list entry gw first, then entries past the grid's warps claimed one at a time (warps past
-    // the list's end leave without touching the counter)
+    pdl_wait();  // taus, row lists and their lengths from the tau kernels
+    // items: the listed rows of the pack's graphs one after another (a list's length is final:
+    // the tau kernel that appends to it has ended)
+    if (threadIdx.x == 0) {
+        uint32_t acc_items = 0;
+        s_pre[0] = 0;
+        for (uint32_t i = 0; i < pk.count; ++i) {
+            const SourceParams<Real, Acc>& gp = pk.g[i];
+            const unsigned total = gp.work[2];
+            acc_items += total > gp.list_base ? min(total - gp.list_base, gp.list_cap) : 0u;
+            s_pre[i + 1] = acc_items;
+        }
+    }
+    __syncthreads();
+    const unsigned nrows = s_pre[pk.count];
+    // item gw first, then items past the grid's warps claimed one at a time (warps past the
+    // end leave without touching the counter)
     const uint64_t nwarps = uint64_t(gridDim.x) * wpb;
     bool first_claim = true;
+    uint32_t last_gi = 0xffffffffu;
     while (true) {
         uint64_t k = gw;
         if (!first_claim) {
             unsigned c = 0;
-            if (lane == 0) c = atomicAdd(p.claim, 1u);
+            if (lane == 0) c = atomicAdd(p0.claim, 1u);
             k = nwarps + __shfl_sync(kFullMask, c, 0);
         }
         first_claim = false;
         if (k >= nrows) break;
+        // the item's graph: the last list whose prefix is at most k (warp-uniform)
+        uint32_t gi = 0;
+        if (Pack::kMax > 1) {
+            uint32_t lo = 0, hi = pk.count;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= k) lo = mid;
+                else hi = mid;
+            }
+            gi = lo;
+        }
+        const SourceParams<Real, Acc>& p = pk.g[gi];
+        if (gi != last_gi) {
+            if (last_gi != 0xffffffffu) flush_stats(pk.g[last_gi].stats);
+            last_gi = gi;
+        }
         if (globaltimer_ns() > deadline) {
             if (lane == 0) atomicOr(p.work + 1, kErrDeadline);
             break;
         }
-        const uint32_t entry = p.list_base + uint32_t(k);
+        const uint32_t n = p.n;
+        const uint32_t* __restrict__ idx = p.idx;
+        const uint32_t* __restrict__ adj = p.adj;
+        const int* __restrict__ taus = p.taus;
+        const uint32_t entry = p.list_base + uint32_t(k - s_pre[gi]);
         const uint32_t src = __ldg(p.rows + entry);
         if (!cleared) {
-            for (uint32_t i = lane; i < n; i += 32) {
+            for (uint32_t i = lane; i < sn; i += 32) {
                 pvec[i] = Real(0);
                 vis[i] = 0;
                 if (JACOBI) fx[i] = 0ull;
@@ -1929,7 +2005,7 @@ source_kernel(SourceParams<Real, Acc> p) {
                     // do not depend on the order.  The touched vertices form the new frontier in
                     // discovery order; once the round is over their residuals become
                     // acc[u] / deg(u) (from_fixed), exactly as push_block_kernel computes them.
-                    unsigned long long* rfx = p.rbuf + gw * size_t(n);
+                    unsigned long long* rfx = p0.rbuf + gw * size_t(sn);
                     pipelined<uint32_t>(qs,
                         [&](uint32_t i0, uint32_t* r) {
 #pragma unroll
@@ -2432,7 +2508,7 @@ source_kernel(SourceParams<Real, Acc> p) {
         if (!SMEM && p.pre) {
             // the residual vector was the block push's column, read in place: the warp's own
             // vector is untouched (and the flags used by the edge bound are back to zero)
-            pvec = p.pvec_g + gw * size_t(n);
+            pvec = p0.pvec_g + gw * size_t(sn);
             lap(7);
             continue;
         }
@@ -2453,24 +2529,8 @@ source_kernel(SourceParams<Real, Acc> p) {
         __syncwarp();
         lap(7);
     }
-    if (!SMEM && lane == 0) p.wclean[gw] = (cleared && !dirty) ? 1 : 0;
-    if (lane == 0) {
-        stat_add(p.stats, kStPushRounds, st_rounds);
-        stat_add(p.stats, kStPushVertices, st_pv);
-        stat_add(p.stats, kStPushTraversals, st_tr);
-    }
-    st_we = warp_sum_u64(st_we);
-    st_wc = warp_sum_u64(st_wc);
-    st_wh = warp_sum_u64(st_wh);
-    st_fb = warp_sum_u64(st_fb);
-    if (lane == 0) {
-        stat_add(p.stats, kStWalkEdges, st_we);
-        stat_add(p.stats, kStWalkCount, st_wc);
-        stat_add(p.stats, kStWalkHops, st_wh);
-        stat_add(p.stats, kStFallback, st_fb);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) stat_add(p.stats, kStPhase0 + i, (unsigned long long)ph[i]);
-    }
+    if (!SMEM && lane == 0) p0.wclean[gw] = (cleared && !dirty) ? 1 : 0;
+    flush_stats(pk.g[last_gi == 0xffffffffu ? 0u : last_gi].stats);
 }
 
 // ---- stage 3: symmetrise (src/aesc.h:532-550) -----------------------------------------------------
@@ -2662,6 +2722,62 @@ int blocks_per_sm(const void* kern, int threads, size_t smem) {
     return per_sm;
 }
 
+// Symmetrisation of one run (stage 3) on the graph's stream.
+template <class Real, class Acc>
+void launch_finish(tgtp_graph* g, float* out) {
+    const RowMarks rm{run_work(g) + 4, g->row_list.as<uint32_t>(), run_work(g) + 2, 1u};
+    ScopedKernel k(g->prof, g->stream, "finish");
+    launch(finish_kernel<Real, Acc>, grid_cap(g->m, 256, g->num_sms, 8), 256, 0, g->stream, true,
+           g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), g->row_of.as<uint32_t>(),
+           g->adjd.as<uint2>(), g->deg.as<uint32_t>(), rm.mark, rm.epoch, g->m, out,
+           g->stats.as<unsigned long long>());
+    TGTP_LAUNCH_CHECK("finish_kernel");
+}
+
+}  // namespace
+
+// ---- batched runs: one persistent source kernel over the rows of many graphs --------------------
+// While a batch is captured (batch.cu), each run_form of a graph whose per-source stage runs as
+// per-warp pushes stops after its tau kernels and leaves that stage and the symmetrisation to the
+// batch: the batch joins every graph's branch, launches one persistent source kernel per
+// (arithmetic form, residual-vector tier) over the listed rows of all its graphs, then launches
+// each graph's finish kernel on the graph's own stream again.  The graphs of a group share one
+// per-warp scratch laid out for the group's largest graph.
+struct BatchEntry {
+    tgtp_graph* g;
+    float* out;
+    int key;    // form_key of the run
+    bool smem;  // residual vectors in shared memory
+    std::vector<unsigned char> params;  // the run's SourceParams<Real, Acc>
+};
+struct BatchGroup {
+    int key;
+    bool smem;
+    std::vector<size_t> members;  // indices into BatchPlan::entries
+    DeviceBuffer scratch, wclean, claims;
+};
+struct BatchPlan {
+    std::vector<BatchEntry> entries;
+    std::vector<std::unique_ptr<BatchGroup>> groups;
+};
+namespace {
+thread_local BatchPlan* t_collect = nullptr;
+
+template <class Real, class Acc>
+bool defer_to_batch(tgtp_graph* g, const tgtp_config& cfg, float* out, bool smem,
+                    const SourceParams<Real, Acc>& p) {
+    if (!t_collect) return false;
+    BatchEntry e;
+    e.g = g;
+    e.out = out;
+    e.key = form_key(cfg);
+    e.smem = smem;
+    e.params.resize(sizeof(p));
+    std::memcpy(e.params.data(), &p, sizeof(p));
+    t_collect->entries.push_back(std::move(e));
+    return true;
+}
+
 // One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
 // JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
 template <class Real, class Acc, bool JACOBI, class Vec>
@@ -2849,8 +2965,9 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         fail(TGTP_ERR_UNSUPPORTED, "source layout does not fit in shared memory");
     const int threads = wpb * 32;
     const size_t smem = use_smem ? per_warp * wpb : size_t(wpb) * kAccBytes;
-    auto kern = use_smem ? source_kernel<Real, Acc, true, JACOBI>
-                         : source_kernel<Real, Acc, false, JACOBI>;
+    using Pack1 = SourcePack<Real, Acc, 1>;
+    auto kern = use_smem ? source_kernel<Real, Acc, true, JACOBI, Pack1>
+                         : source_kernel<Real, Acc, false, JACOBI, Pack1>;
     const int per_sm = blocks_per_sm(reinterpret_cast<const void*>(kern), threads, smem);
     if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "source kernel does not fit on an SM");
     uint64_t blocks = uint64_t(g->num_sms) * per_sm;
@@ -2912,12 +3029,17 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.pre_cols = nullptr;
     p.pre_final = nullptr;
     p.multi = multi;
+    p.scratch_n = uint32_t(n);
+    Pack1 pk;
+    pk.count = 1;
     if (!block_mode) {
         p.claim = work;
         p.list_base = 0;
         p.list_cap = uint32_t(n);
+        if (defer_to_batch<Real, Acc>(g, cfg, out, use_smem, p)) return;
+        pk.g[0] = p;
         ScopedKernel k(g->prof, s, "source");
-        launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
+        launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, pk);
         TGTP_LAUNCH_CHECK("source_kernel");
     } else if constexpr (JACOBI) {  // the block push exists for the mixed form only
         grow(g, g->block_cols, 2 * size_t(n) * kBlockCols * sizeof(float) * block_ctas);
@@ -2998,21 +3120,148 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             p.claim = claims + w;
             p.list_base = bp.base;
             p.list_cap = block_ctas * kBlockCols;
+            pk.g[0] = p;
             ScopedKernel k(g->prof, s, "source");
-            launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, p);
+            launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, pk);
             TGTP_LAUNCH_CHECK("source_kernel");
         }
     }
-    {
-        ScopedKernel k(g->prof, s, "finish");
-        launch(finish_kernel<Real, Acc>, grid_cap(m, 256, g->num_sms, 8), 256, 0, s, true,
-            g->preds.as<Acc>(), g->sym_src.as<uint32_t>(), g->row_of.as<uint32_t>(),
-            g->adjd.as<uint2>(), g->deg.as<uint32_t>(), rm.mark, rm.epoch, m, out, stats);
-        TGTP_LAUNCH_CHECK("finish_kernel");
+    launch_finish<Real, Acc>(g, out);
+}
+
+// The persistent source kernel of one batch group: per-warp scratch for the group's largest
+// graph, packs of up to kBatchPack graphs, each pack one launch on `s` with its own claim counter.
+template <class Real, class Acc, bool SMEM, bool JACOBI>
+void launch_group(BatchPlan& plan, BatchGroup& grp, cudaStream_t s, int num_sms) {
+    using Pack = SourcePack<Real, Acc, kBatchPack>;
+    static_assert(sizeof(Pack) < 32000, "pack must fit in the kernel parameter space");
+    uint32_t sn = 1, maxd = 1;
+    uint64_t rows = 0;
+    for (size_t i : grp.members) {
+        const tgtp_graph* g = plan.entries[i].g;
+        sn = std::max<uint32_t>(sn, uint32_t(g->n));
+        maxd = std::max<uint32_t>(maxd, g->max_degree);
+        rows += g->n;
+    }
+    const size_t pv_bytes = (size_t(sn) * sizeof(Real) + 15) & ~size_t(15);
+    const size_t vis_bytes = (size_t(sn) + 15) & ~size_t(15);
+    const size_t fx_bytes = JACOBI ? sizeof(unsigned long long) * size_t(sn) : 0;
+    const bool fx_in_smem = SMEM && JACOBI &&
+                            pv_bytes + vis_bytes + fx_bytes + kAccBytes <= size_t(112) * 1024;
+    const size_t per_warp = pv_bytes + vis_bytes + (fx_in_smem ? fx_bytes : 0) + kAccBytes;
+    const int wpb = SMEM ? 1 : 4;
+    const int threads = 32 * wpb;
+    const size_t smem = SMEM ? per_warp * wpb : size_t(wpb) * kAccBytes;
+    auto kern = source_kernel<Real, Acc, SMEM, JACOBI, Pack>;
+    const int per_sm = blocks_per_sm(reinterpret_cast<const void*>(kern), threads, smem);
+    if (per_sm < 1) fail(TGTP_ERR_UNSUPPORTED, "batch source kernel does not fit on an SM");
+    uint64_t blocks = std::min<uint64_t>(uint64_t(num_sms) * per_sm, (rows + wpb - 1) / wpb);
+    blocks = std::max<uint64_t>(blocks, 1);
+    const uint64_t warps = blocks * wpb;
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t q_bytes = align(warps * 2 * size_t(sn) * 4);
+    const size_t it_bytes = align(warps * maxd * sizeof(WalkItem));
+    const size_t rb_bytes = JACOBI ? align(warps * size_t(sn) * sizeof(unsigned long long)) : 0;
+    const size_t pvg_bytes = SMEM ? 0 : align(warps * size_t(sn) * sizeof(Real));
+    const size_t visg_bytes = SMEM ? 0 : align(warps * vis_bytes);
+    const size_t fxg_bytes = (JACOBI && !fx_in_smem) ? align(warps * fx_bytes) : 0;
+    grp.scratch.reserve(q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
+    grp.wclean.reserve(warps + 16);
+    const size_t packs = (grp.members.size() + kBatchPack - 1) / kBatchPack;
+    grp.claims.reserve(sizeof(unsigned) * (packs + 1));
+    unsigned char* base = grp.scratch.as<unsigned char>();
+    // each replay starts from "vectors not known to be zero" and fresh claim counters
+    TGTP_CUDA(cudaMemsetAsync(grp.wclean.ptr, 0, warps + 16, s));
+    TGTP_CUDA(cudaMemsetAsync(grp.claims.ptr, 0, sizeof(unsigned) * (packs + 1), s));
+    for (size_t pk0 = 0; pk0 < grp.members.size(); pk0 += kBatchPack) {
+        Pack pk;
+        pk.count = uint32_t(std::min<size_t>(kBatchPack, grp.members.size() - pk0));
+        for (uint32_t j = 0; j < pk.count; ++j) {
+            SourceParams<Real, Acc> p;
+            std::memcpy(&p, plan.entries[grp.members[pk0 + j]].params.data(), sizeof(p));
+            unsigned char* b = base;
+            p.qbuf = reinterpret_cast<uint32_t*>(b);
+            b += q_bytes;
+            p.items = reinterpret_cast<WalkItem*>(b);
+            b += it_bytes;
+            p.rbuf = JACOBI ? reinterpret_cast<unsigned long long*>(b) : nullptr;
+            b += rb_bytes;
+            p.pvec_g = SMEM ? nullptr : reinterpret_cast<Real*>(b);
+            b += pvg_bytes;
+            p.vis_g = SMEM ? nullptr : b;
+            b += visg_bytes;
+            p.fx_g = fxg_bytes ? reinterpret_cast<unsigned long long*>(b) : nullptr;
+            p.wclean = grp.wclean.as<unsigned char>();
+            p.vis_stride = vis_bytes;
+            p.smem_per_warp = per_warp;
+            p.max_degree = maxd;
+            p.scratch_n = sn;
+            p.claim = grp.claims.as<unsigned>() + pk0 / kBatchPack;
+            pk.g[j] = p;
+        }
+        launch(kern, unsigned(blocks), unsigned(threads), smem, s, false, pk);
+        TGTP_LAUNCH_CHECK("source_kernel (batch)");
     }
 }
 
 }  // namespace
+
+BatchPlan* batch_plan_new() { return new BatchPlan(); }
+void batch_plan_free(BatchPlan* plan) { delete plan; }
+void batch_plan_collect(BatchPlan* plan) {
+    if (plan) plan->entries.clear();
+    t_collect = plan;
+}
+
+size_t batch_plan_deferred(const BatchPlan* plan) { return plan->entries.size(); }
+
+void batch_plan_launch(BatchPlan* plan, cudaStream_t s, int num_sms) {
+    plan->groups.clear();
+    for (size_t i = 0; i < plan->entries.size(); ++i) {
+        const BatchEntry& e = plan->entries[i];
+        BatchGroup* grp = nullptr;
+        for (auto& g : plan->groups)
+            if (g->key == e.key && g->smem == e.smem) grp = g.get();
+        if (!grp) {
+            plan->groups.push_back(std::make_unique<BatchGroup>());
+            grp = plan->groups.back().get();
+            grp->key = e.key;
+            grp->smem = e.smem;
+        }
+        grp->members.push_back(i);
+    }
+    for (auto& grp : plan->groups) {
+        switch (grp->key) {
+            case 0:
+                if (grp->smem) launch_group<float, float, true, false>(*plan, *grp, s, num_sms);
+                else launch_group<float, float, false, false>(*plan, *grp, s, num_sms);
+                break;
+            case 1:
+                if (grp->smem) launch_group<double, double, true, false>(*plan, *grp, s, num_sms);
+                else launch_group<double, double, false, false>(*plan, *grp, s, num_sms);
+                break;
+            default:
+                if (grp->smem) launch_group<float, double, true, true>(*plan, *grp, s, num_sms);
+                else launch_group<float, double, false, true>(*plan, *grp, s, num_sms);
+                break;
+        }
+    }
+}
+
+void batch_plan_finish(BatchPlan* plan) {
+    for (const BatchEntry& e : plan->entries) {
+        if (e.key == 0) launch_finish<float, float>(e.g, e.out);
+        else if (e.key == 1) launch_finish<double, double>(e.g, e.out);
+        else launch_finish<float, double>(e.g, e.out);
+    }
+}
+
+std::vector<tgtp_graph*> batch_plan_graphs(const BatchPlan* plan) {
+    std::vector<tgtp_graph*> v;
+    for (const BatchEntry& e : plan->entries) v.push_back(e.g);
+    return v;
+}
+
 
 void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
     if (!(cfg.epsilon > 0 && cfg.epsilon < 1))

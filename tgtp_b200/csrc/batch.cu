@@ -3,13 +3,20 @@
 // A batch is built once: every run is executed once on its graph handle (which sizes all of the
 // handle's buffers and weight tables, and optionally times the candidate source-kernel layouts and
 // keeps the fastest), then all runs are captured from one origin stream that forks to each handle's
-// stream and joins back, so runs on different graphs are parallel branches of the CUDA graph and
-// their kernels (tau, source, finish of every graph) overlap on the device.  tgtp_batch_run is one
+// stream.  Each graph's branch runs its tau kernels; the per-source stage of every run that pushes
+// per warp is left to the batch (aesc.cu, BatchPlan): the branches join, one persistent source
+// kernel per (arithmetic form, residual-vector tier) works through the listed rows of all those
+// graphs as one queue of (graph, row) items, so the rows of small graphs fill the SMs that a large
+// graph leaves idle, and the branches fork again for each graph's symmetrisation.  Runs whose push
+// is the multi-source block push keep their whole run in their branch.  tgtp_batch_run is one
 // cudaGraphLaunch.  While a batch is alive its graphs keep their buffers: runs on them that would
-// need larger buffers, eigen uploads and frees are refused.
+// need larger buffers, eigen uploads and frees are refused.  TGTP_BATCH_PERSISTENT=0 captures every
+// run whole in its branch instead (no shared persistent kernel).
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 #include <set>
+#include <string>
 #include <vector>
 
 #include "internal.hpp"
@@ -23,12 +30,14 @@ struct tgtp_batch {
     cudaStream_t last = nullptr;  // stream of the last launch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    tgtp::BatchPlan* plan = nullptr;  // the deferred per-source stages and their shared scratch
 
     ~tgtp_batch() {
         if (last) cudaStreamSynchronize(last);
         if (origin) cudaStreamSynchronize(origin);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (plan) tgtp::batch_plan_free(plan);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         if (origin) tgtp::stream_release(origin);
         for (tgtp_graph* g : graphs) --g->batch_refs;
@@ -61,12 +70,37 @@ void capture(tgtp_batch* b) {
         cudaEvent_t fork = new_event(b);
         TGTP_CUDA(cudaEventRecord(fork, b->origin));
         for (cudaStream_t s : streams) TGTP_CUDA(cudaStreamWaitEvent(s, fork, 0));
-        for (size_t i = 0; i < b->graphs.size(); ++i)
-            aesc_run(b->graphs[i], b->configs[i], b->outs[i]);
-        for (cudaStream_t s : streams) {
-            cudaEvent_t join = new_event(b);
-            TGTP_CUDA(cudaEventRecord(join, s));
-            TGTP_CUDA(cudaStreamWaitEvent(b->origin, join, 0));
+        const char* pe = std::getenv("TGTP_BATCH_PERSISTENT");
+        const bool persistent = !(pe && std::string(pe) == "0");
+        if (persistent) {
+            if (!b->plan) b->plan = batch_plan_new();
+            batch_plan_collect(b->plan);
+        }
+        try {
+            for (size_t i = 0; i < b->graphs.size(); ++i)
+                aesc_run(b->graphs[i], b->configs[i], b->outs[i]);
+        } catch (...) {
+            batch_plan_collect(nullptr);
+            throw;
+        }
+        batch_plan_collect(nullptr);
+        auto join_all = [&]() {
+            for (cudaStream_t s : streams) {
+                cudaEvent_t join = new_event(b);
+                TGTP_CUDA(cudaEventRecord(join, s));
+                TGTP_CUDA(cudaStreamWaitEvent(b->origin, join, 0));
+            }
+        };
+        join_all();
+        if (persistent && batch_plan_deferred(b->plan) > 0) {
+            // the persistent source kernels on the origin stream, then every deferred graph's
+            // symmetrisation on its own stream again
+            batch_plan_launch(b->plan, b->origin, b->graphs[0]->num_sms);
+            cudaEvent_t fork2 = new_event(b);
+            TGTP_CUDA(cudaEventRecord(fork2, b->origin));
+            for (cudaStream_t s : streams) TGTP_CUDA(cudaStreamWaitEvent(s, fork2, 0));
+            batch_plan_finish(b->plan);
+            join_all();
         }
     } catch (...) {
         cudaGraph_t dead = nullptr;

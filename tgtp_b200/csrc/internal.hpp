@@ -215,4 +215,17 @@ void aesc_check_flags(tgtp_graph* g);
 constexpr int kRunStatSlots = 32;
 void aesc_read_stats(tgtp_graph* g, unsigned long long* st);
 void graph_prepare(tgtp_graph* g);
+// Batched runs (aesc.cu): while collection is on for this thread (batch_plan_collect(plan)),
+// aesc_run leaves the per-source stage and the symmetrisation of per-warp-push runs to the plan;
+// batch_plan_launch then runs one persistent source kernel per (form, tier) group over all the
+// deferred graphs' rows on stream s, and batch_plan_finish each deferred graph's finish kernel on
+// the graph's own stream.  batch_plan_collect(nullptr) ends collection.
+struct BatchPlan;
+BatchPlan* batch_plan_new();
+void batch_plan_free(BatchPlan* plan);
+void batch_plan_collect(BatchPlan* plan);
+size_t batch_plan_deferred(const BatchPlan* plan);
+void batch_plan_launch(BatchPlan* plan, cudaStream_t s, int num_sms);
+void batch_plan_finish(BatchPlan* plan);
+std::vector<tgtp_graph*> batch_plan_graphs(const BatchPlan* plan);
 }  // namespace tgtp
