@@ -351,26 +351,22 @@ def sparse_inputs(root: str):
     return g, values, v32, v64
 
 
-def run_batch_workload(args):
-    """64 seeded graphs of uneven size (n log-uniform in [1,000, 200,000]; Chung-Lu exponent
-    2.1-2.8, R-MAT a=0.57, 2-D grid with chords; average degree 8-40), each with its own epsilon
-    from {0.05, 0.01, 0.005}, omega=128, gamma=10; eigenpairs from the GPU eigen prep.  value =
-    sum of undirected edges / device time of one replay of the batched mixed form (BF16 vectors),
-    against the same graphs run one after another in the plain FP64 form (each run timed on its
-    own, synchronised).  The inputs are far larger than L2 (per-source residual blocks of GBs),
-    so no flush is needed between steps."""
+def batch_measure(work, steps: int, accuracy_slots: int = 0) -> dict:
+    """The batched form against one-by-one runs on `work` = [(EdgeList, eps)]: eigenpairs from the
+    GPU eigen prep; every graph in the plain FP64 form one after another (each run timed by CUDA
+    events on one stream), the mixed form (BF16 vectors) the same way, then the mixed form as one
+    batch (one CUDA graph whose per-source stage is one persistent launch over all graphs' rows),
+    `steps` timed replays after one untimed.  With accuracy_slots > 0, the fraction of that many
+    sampled edges per graph within the graph's epsilon of the exact spanning centrality (the
+    library's GPU conjugate-gradient solver), for both forms."""
     import numpy as np
     import torch
 
-    from tgtp_b200 import eigenprep_gpu, synth
+    from tgtp_b200 import eigenprep_gpu
     from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, Batch, PRECISION_FP64,
-                                PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64)
+                                PRECISION_MIXED, VEC_BF16, VEC_F32, VEC_F64, exact_sc_slots)
 
-    rank, world, local = replicas.rank_info()
-    torch.cuda.set_device(local)
-    os.environ.setdefault("TGTP_KERNEL_DEADLINE_S", "300")
     t0 = time.perf_counter()
-    work = synth.config5_graphs(replicas.workload_seed(5, rank), 64)
     graphs = []
     for g, eps in work:
         vals, vecs, _, _, _ = eigenprep_gpu.compute(g.n, g.u, g.v, OMEGA, seed=1, tol=1e-6,
@@ -385,7 +381,6 @@ def run_batch_workload(args):
     prep_s = time.perf_counter() - t0
     E = sum(g.num_edges for g, _, _ in graphs)
     outs = [torch.empty(dg.m, dtype=torch.float32, device="cuda") for _, _, dg in graphs]
-
     stream = torch.cuda.Stream()
 
     def one_by_one(cfgs):
@@ -414,11 +409,10 @@ def run_batch_workload(args):
     fp64 = [o.cpu().numpy().copy() for o in outs]
     runs, mixed_secs = one_by_one(mixed_cfgs)
     b = Batch([(a, o.data_ptr()) for a, o in zip(runs, outs)])
-    steps = max(1, min(args.steps, 3))
     b.run(stream.cuda_stream)
     b.wait()
     times = []
-    for _ in range(steps):
+    for _ in range(max(1, steps)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         b.run(stream.cuda_stream)
@@ -426,18 +420,75 @@ def run_batch_workload(args):
         b.wait()
         times.append(e0.elapsed_time(e1) * 1e-3)
     batch_s = float(np.median(times))
-    dev = np.concatenate([np.abs(o.cpu().numpy().astype(np.float64) - f) / np.abs(f)
-                          for o, f in zip(outs, fp64)])
+    mixed = [o.cpu().numpy().copy() for o in outs]
+    dev = np.concatenate([np.abs(m.astype(np.float64) - f) / np.abs(f)
+                          for m, f in zip(mixed, fp64)])
     b.free()
+    out = {"graphs": len(graphs), "undirected_edges": E, "vertices": sum(g.n for g, _, _ in graphs),
+           "batched_mixed_seconds": batch_s, "batched_mixed_edges_per_s": E / batch_s,
+           "fp64_one_by_one": {"edges_per_s": E / sum(fp64_secs), "seconds": sum(fp64_secs),
+                               "slowest": sorted(((round(s, 3), g.name, eps) for s, (g, eps, _)
+                                                  in zip(fp64_secs, graphs)), reverse=True)[:3]},
+           "mixed_one_by_one": {"edges_per_s": E / sum(mixed_secs), "seconds": sum(mixed_secs)},
+           "speedup_batched_mixed_vs_fp64_one_by_one": sum(fp64_secs) / batch_s,
+           "mixed_vs_fp64_rel_dev": {"median": float(np.median(dev)),
+                                     "p99": float(np.percentile(dev, 99)),
+                                     "max": float(dev.max())},
+           "input_prep_s": prep_s}
+    if accuracy_slots:
+        rng = np.random.default_rng(7)
+        per_graph, tot = [], {"fp64": 0, "mixed": 0, "slots": 0}
+        for (g, eps, dg), f, m in zip(graphs, fp64, mixed):
+            idx, adj = g.csr()
+            rows = np.repeat(np.arange(g.n), np.diff(idx.astype(np.int64)))
+            fwd = np.flatnonzero(adj.astype(np.int64) > rows)
+            slots = np.sort(rng.choice(fwd, size=min(accuracy_slots, len(fwd)),
+                                       replace=False)).astype(np.uint32)
+            exact, _ = exact_sc_slots(dg, slots, tol=1e-9)
+            wf = int(np.sum(np.abs(f[slots] - exact) <= eps))
+            wm = int(np.sum(np.abs(m[slots] - exact) <= eps))
+            per_graph.append({"graph": g.name, "n": g.n, "eps": eps, "slots": len(slots),
+                              "fp64_within_eps": wf / len(slots),
+                              "mixed_within_eps": wm / len(slots)})
+            tot["fp64"] += wf
+            tot["mixed"] += wm
+            tot["slots"] += len(slots)
+        out["accuracy_vs_exact_sc"] = {
+            "sampled_edges": tot["slots"], "fp64_within_eps": tot["fp64"] / tot["slots"],
+            "mixed_within_eps": tot["mixed"] / tot["slots"], "per_graph": per_graph,
+            "exact": "tgtp_exact_sc_slots (FP64 conjugate gradients, tol 1e-9)"}
+    for _, _, dg in graphs:
+        dg.free()
+    return out
+
+
+def run_batch_workload(args):
+    """64 seeded graphs of uneven size (n log-uniform in [1,000, 200,000]; Chung-Lu exponent
+    2.1-2.8, R-MAT a=0.57, 2-D grid with chords; average degree 8-40), each with its own epsilon
+    from {0.05, 0.01, 0.005}, omega=128, gamma=10.  value = sum of undirected edges / device time
+    of one replay of the batched mixed form (BF16 vectors), against the same graphs run one after
+    another in the plain FP64 form (see batch_measure).  The inputs are far larger than L2
+    (per-source residual blocks of GBs), so no flush is needed between steps."""
+    import torch
+
+    from tgtp_b200 import synth
+
+    rank, world, local = replicas.rank_info()
+    torch.cuda.set_device(local)
+    os.environ.setdefault("TGTP_KERNEL_DEADLINE_S", "300")
+    work = synth.config5_graphs(replicas.workload_seed(5, rank), 64)
+    steps = max(1, min(args.steps, 3))
+    r = batch_measure(work, steps)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    batch_s, fp64_total = replicas.slowest([batch_s, sum(fp64_secs)], device="cuda")
+    batch_s, fp64_total = replicas.slowest([r["batched_mixed_seconds"],
+                                            r["fp64_one_by_one"]["seconds"]], device="cuda")
     if rank == 0:
-        hbm, peak_kind = peaks()
+        E = r["undirected_edges"]
         line = {
             "metric": METRIC, "value": replicas.job_rate(E, batch_s, world), "unit": "edges/s",
             "n_gpus": world,
@@ -447,22 +498,12 @@ def run_batch_workload(args):
             "config": {"workload": "batched AESC: 64 graphs, n log-uniform in [1e3, 2e5], "
                                    "Chung-Lu / R-MAT / grid+chords, avg degree 8-40, own eps "
                                    "from {0.05, 0.01, 0.005}, omega=128, gamma=10",
-                       "undirected_edges": E, "vertices": sum(g.n for g, _, _ in graphs),
+                       "undirected_edges": E, "vertices": r["vertices"],
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
-            "fp64_one_by_one": {"edges_per_s": replicas.job_rate(E, fp64_total, world),
-                                "seconds": fp64_total,
-                                "slowest": sorted(((round(s, 3), g.name, eps) for s, (g, eps, _)
-                                                   in zip(fp64_secs, graphs)), reverse=True)[:3]},
-            "mixed_one_by_one": {"edges_per_s": E / sum(mixed_secs), "seconds": sum(mixed_secs)},
+            **{k: v for k, v in r.items() if k not in ("undirected_edges", "vertices")},
             "speedup_batched_mixed_vs_fp64_one_by_one": fp64_total / batch_s,
-            "mixed_vs_fp64_rel_dev": {"median": float(np.median(dev)),
-                                      "p99": float(np.percentile(dev, 99)),
-                                      "max": float(dev.max())},
-            "input_prep_s": prep_s,
         }
         print(json.dumps(line))
-    for _, _, dg in graphs:
-        dg.free()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
@@ -508,6 +549,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmat", action="store_true", help="skip the R-MAT scale-18 walk line")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 16-graph batched-form measurement")
     ap.add_argument("--no-push", action="store_true",
                     help="skip the push-bound tgtp measurements (eps 0.01 / 0.005, sparse graph)")
     ap.add_argument("--workload", choices=["aesc", "batch"], default="aesc",
@@ -681,6 +724,16 @@ def main():
         if not args.no_rmat:
             saba["rmat18"] = saba_rmat18(hbm, peak_kind, root, not args.no_cpu_baseline)
 
+        # ---- the batched form on the 16 smallest graphs of the batched workload ----
+        batch16 = None
+        if not args.no_batch:
+            from tgtp_b200 import synth
+
+            work = sorted(synth.config5_graphs(5, 64), key=lambda ge: ge[0].n)[:16]
+            batch16 = {"workload": "the 16 smallest of the 64 batched-workload graphs (seed 5), "
+                                   "own eps each, omega=128, gamma=10",
+                       **batch_measure(work, 3, accuracy_slots=256)}
+
         # ---- tgtp where the push and the walks run ----
         push = {}
         if not args.no_push:
@@ -738,6 +791,7 @@ def main():
                          for k, v in mixed.items()}},
             "saba": saba,
             "push_bound": push,
+            "batch16": batch16,
             "wall_s_timed_region": wall64,
         }
         print(json.dumps(line))
