@@ -149,10 +149,13 @@ tgtp_status tgtp_last_run_stats(tgtp_graph* g, tgtp_run_stats* out);
 tgtp_status tgtp_last_taus(tgtp_graph* g, int32_t* host_taus);
 
 /* Times the candidate layouts of the source kernel (per-source residual vectors in shared memory
- * or in HBM, warps per block) for cfg's precision form on this graph, `trials` runs each after a
+ * or in HBM, warps per block; for the mixed form also the multi-source block push at four
+ * push-frontier thresholds) for cfg's precision form on this graph, `trials` runs each after a
  * warm-up, and keeps the fastest on the handle for later runs of that form.  Scores are identical
  * under every layout.  *layout (may be NULL) receives the choice: 0x100 bit = shared memory, low
- * byte = warps per block.  The reference has no counterpart (its OpenMP loop has one layout). */
+ * byte = warps per block, 0x200 = block push, bits 12-13 = its compaction threshold (a round is
+ * compacted to the rows next to the live ones when their degree sum is below m / 4, m / 2,
+ * m / 16, or never).  The reference has no counterpart (its OpenMP loop has one layout). */
 tgtp_status tgtp_graph_tune(tgtp_graph* g, const tgtp_config* cfg, float* device_scores,
                             int32_t trials, int32_t* layout);
 
@@ -183,6 +186,15 @@ tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t
 /* Counters into caller-owned device memory (n uint32), asynchronous on the handle's stream. */
 tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
                               uint32_t* device_counters);
+
+/* Times the walk layouts for this graph and walk configuration and keeps the fastest on the handle
+ * for later saba_count calls: 1, 2 or 4 walkers per lane (4, 8 or 16 eight-lane bouquets per warp)
+ * over the degree-renumbered walk copy, plain or with the next row's record inlined in each slot.
+ * `trials` timed runs each after a warm-up.  *choice (may be NULL) receives the pick: low byte =
+ * walkers per lane, 0x100 = inlined copy.  Counters are identical under every layout.  The
+ * reference has no counterpart (its OpenMP loop has one layout). */
+tgtp_status saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t trials,
+                      int32_t* choice);
 
 /* No counterpart in the reference: the walk counter for callers that cannot allocate device
  * memory, e.g. a process whose device memory is owned by another allocator or budget, or a

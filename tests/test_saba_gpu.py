@@ -173,3 +173,39 @@ def test_saba_rmat18_static_entry_point_matches_the_fixture(cuda_device, rmat18,
                                             C.c_void_p(d_adj.data_ptr()), rmat18["g"].n, depth,
                                             walks, None, C.byref(res)))
     assert (int(res.visit_count), int(res.checksum)) == (cell["visit_count"], cell["checksum"])
+
+
+def test_saba_tuned_layout_gives_the_same_counters(cuda_device, oracle_lib):
+    """saba_tune times 1 / 2 / 4 walkers per lane over the plain and the inlined walk copy and
+    keeps the fastest; every layout, and so the chosen one, gives the oracle's counters."""
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count, saba_tune
+
+    g = synth.rmat(15, 8, 0.57, 0.19, 0.19, 9)
+    idx, adj = g.csr()
+    want = oracle_lib.saba(idx, adj, 7, 32)
+    dg = AESCGraph.from_csr(idx, adj)
+    choice = saba_tune(dg, 7, 32, trials=1)
+    assert (choice & 0xff) in (1, 2, 4) and (choice & ~0x1ff) == 0
+    counts, visits, _, _ = saba_count(dg, 7, 32)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    assert visits == g.n * 32 * 7
+    dg.free()
+
+
+@pytest.mark.parametrize("inline", ["0", "1"])
+@pytest.mark.parametrize("wpl", ["1", "2", "4"])
+def test_saba_every_walk_layout_matches_the_oracle(cuda_device, oracle_lib, monkeypatch, inline,
+                                                   wpl):
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    monkeypatch.setenv("TGTP_SABA_INLINE", inline)
+    monkeypatch.setenv("TGTP_SABA_WPL", wpl)
+    g = synth.rmat(14, 8, 0.57, 0.19, 0.19, 3)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, checksum, _ = saba_count(dg, 10, 64)
+    want = oracle_lib.saba(idx, adj, 10, 64)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    dg.free()

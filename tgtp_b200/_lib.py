@@ -77,6 +77,7 @@ SIGNATURES = {
     "tgtp_last_taus": (C.c_int, [_vp, _vp]),
     "saba_count": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _vp, C.POINTER(SabaResult)]),
     "saba_count_device": (C.c_int, [_vp, C.c_uint32, C.c_uint32, _vp]),
+    "saba_tune": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_int32)]),
     "tgtp_exact_sc_slots": (C.c_int, [_vp, _vp, C.c_uint32, C.c_double, C.c_uint32, _vp, _vp]),
     "saba_count_static": (C.c_int, [_vp, _vp, _u64, C.c_uint32, C.c_uint32, _vp,
                                     C.POINTER(SabaResult)]),

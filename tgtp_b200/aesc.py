@@ -229,6 +229,14 @@ def saba_count(g: AESCGraph, depth: int, n_walks: int, counters: bool = True):
     return out, int(res.visit_count), int(res.checksum), int(res.fallback_bouquets)
 
 
+def saba_tune(g: AESCGraph, depth: int, n_walks: int, trials: int = 3) -> int:
+    """Times the walk layouts for this graph and configuration and keeps the fastest on the
+    handle; returns the choice (low byte: walkers per lane, 0x100: inlined walk copy)."""
+    choice = C.c_int32(0)
+    check(lib().saba_tune(g.handle, depth, n_walks, trials, C.byref(choice)))
+    return int(choice.value)
+
+
 def exact_sc_slots(g: AESCGraph, slots, tol: float = 1e-10, max_iter: int = 20000):
     """Exact spanning centrality (effective resistance) of the given CSR slots on the device:
     (resistances float64[len(slots)], iterations per batch of 32 slots)."""

@@ -76,6 +76,17 @@ static_assert(kStCount <= kRunStatSlots, "aesc_read_stats writes kStCount counte
 // warps per block; 0 = the default rule.
 constexpr uint16_t kLayoutSmem = 0x100;
 constexpr uint16_t kLayoutBlock = 0x200;  // mixed form: multi-source block push
+// block push: the frontier size below which a round is compacted, as m / list_div, in bits 12-13
+// (0 = the default list_div of 4, 1 = 2, 2 = 16, 3 = never compacted)
+constexpr int kLayoutListShift = 12;
+inline uint32_t layout_list_div(uint16_t layout) {
+    switch ((layout >> kLayoutListShift) & 3) {
+        case 1: return 2;
+        case 2: return 16;
+        case 3: return 0;
+        default: return 4;
+    }
+}
 inline int form_key(const tgtp_config& cfg) {
     if (cfg.precision == TGTP_PRECISION_FP32) return 0;
     if (cfg.precision == TGTP_PRECISION_FP64) return 1;
@@ -3075,12 +3086,13 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         grow(g, g->block_lists, sizeof(uint32_t) * 4 * size_t(n) * block_ctas + 16);
         bp.lists = g->block_lists.as<uint32_t>();
         bp.m = m;
-        // a round is compacted when its live rows' degree sum is below m / list_div
-        // (TGTP_BLOCK_LIST_DIV); TGTP_BLOCK_ROUNDS=compact|full fixes the choice (the values do
-        // not depend on it)
-        bp.list_div = 4;
-        if (const char* e = std::getenv("TGTP_BLOCK_LIST_DIV")) bp.list_div = uint32_t(std::atoi(e));
-        bp.rounds_mode = 0;
+        // a round is compacted when its live rows' degree sum is below m / list_div (the tuned
+        // layout's threshold, else TGTP_BLOCK_LIST_DIV, else 4); TGTP_BLOCK_ROUNDS=compact|full
+        // fixes the choice (the values do not depend on it)
+        bp.list_div = layout_list_div(g->src_layout[key]);
+        if (const char* e = std::getenv("TGTP_BLOCK_LIST_DIV"))
+            if (!g->src_layout[key]) bp.list_div = uint32_t(std::atoi(e));
+        bp.rounds_mode = bp.list_div == 0 ? 2 : 0;
         if (const char* e = std::getenv("TGTP_BLOCK_ROUNDS")) {
             if (std::string(e) == "compact") bp.rounds_mode = 1;
             else if (std::string(e) == "full") bp.rounds_mode = 2;
@@ -3355,9 +3367,11 @@ int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int t
     for (int w : {1, 2})
         if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(kLayoutSmem | w));
     for (int w : {1, 2, 4}) cand.push_back(uint16_t(w));
-    if (mixed) {  // the block push, with the per-source stage in the best layout that fits
+    if (mixed) {  // the block push, with the per-source stage in the best layout that fits,
+                  // at each compaction threshold
         const uint16_t post = per_warp <= size_t(112) * 1024 ? uint16_t(kLayoutSmem | 1) : uint16_t(4);
-        cand.push_back(uint16_t(kLayoutBlock | post));
+        for (int ld = 0; ld < 4; ++ld)
+            cand.push_back(uint16_t(kLayoutBlock | post | (ld << kLayoutListShift)));
     }
     cudaEvent_t e0, e1;
     TGTP_CUDA(cudaEventCreate(&e0));

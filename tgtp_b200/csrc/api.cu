@@ -619,6 +619,18 @@ tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
     });
 }
 
+tgtp_status saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t trials,
+                      int32_t* choice) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        if (n_walks % 8 != 0)
+            fail(TGTP_ERR_INVALID_ARGUMENT,
+                 "n_walks must be a multiple of 8 within the 32-bit grid domain");
+        const int pick = tgtp::saba_tune(g, depth, n_walks, trials);
+        if (choice) *choice = pick;
+    });
+}
+
 tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* host_counters,
                        saba_result* out) {
     return guarded([&] {

@@ -192,6 +192,9 @@ struct tgtp_graph {
     // the first saba_count that walks the inlined copy)
     tgtp::DeviceBuffer saba_adj16;
     bool saba_inline_ready = false;
+    // the walk layout saba_tune chose: walkers per lane (low byte: 1, 2 or 4, so 4, 8 or 16
+    // bouquets per warp) and 0x100 for the inlined copy; 0 = not tuned
+    uint16_t saba_choice = 0;
     int32_t last_precision = -1;
     bool have_run = false;
 
@@ -202,6 +205,9 @@ struct tgtp_graph {
 
 namespace tgtp {
 void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_counters);
+// Times the walk layouts (walkers per lane 1 / 2 / 4, plain or inlined copy) for this graph and
+// walk configuration, `trials` runs each after a warm-up, and keeps the fastest on the handle.
+int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials);
 void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* host_sums3);
 void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores);
 // Times the candidate source-kernel layouts of cfg's form on this graph (trials runs each, after

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -434,9 +435,12 @@ void saba_prepare(tgtp_graph* g) {
 // Whether saba_count walks the inlined copy (one dependent 16-byte load per hop) or the plain
 // renumbered copy (two): TGTP_SABA_INLINE=0/1 decides, else the inlined copy is used while its
 // 16 bytes per slot stay within 2 GiB.
+bool saba_inline_fits(const tgtp_graph* g) { return g->m * sizeof(uint4) <= (size_t(2) << 30); }
+
 bool saba_use_inline(const tgtp_graph* g) {
+    if (g->saba_choice) return (g->saba_choice & 0x100) != 0;
     if (const char* e = std::getenv("TGTP_SABA_INLINE")) return std::atoi(e) != 0;
-    return g->m * sizeof(uint4) <= (size_t(2) << 30);
+    return saba_inline_fits(g);
 }
 
 void saba_prepare_inline(tgtp_graph* g) {
@@ -502,7 +506,8 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
     auto* cnt = g->saba_cnt.as<uint32_t>();
     TGTP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * g->n, s));
     int wpl = 1;
-    if (const char* e = std::getenv("TGTP_SABA_WPL")) wpl = std::atoi(e);
+    if (g->saba_choice) wpl = g->saba_choice & 0xff;
+    else if (const char* e = std::getenv("TGTP_SABA_WPL")) wpl = std::atoi(e);
     switch (wpl) {
         case 2: saba_launch<2>(g, depth, bouquets_per_src, grid_step, total, cnt, sums + 2); break;
         case 4: saba_launch<4>(g, depth, bouquets_per_src, grid_step, total, cnt, sums + 2); break;
@@ -515,6 +520,54 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
                                                         device_counters);
         TGTP_LAUNCH_CHECK("saba_scatter_kernel");
     }
+}
+
+int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials) {
+    std::vector<uint16_t> cand;
+    for (int inl : {1, 0}) {
+        if (inl && !saba_inline_fits(g)) continue;
+        for (int wpl : {1, 2, 4}) cand.push_back(uint16_t((inl ? 0x100 : 0) | wpl));
+    }
+    g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
+    auto* c = g->counters.as<uint32_t>();
+    cudaEvent_t e0, e1;
+    TGTP_CUDA(cudaEventCreate(&e0));
+    TGTP_CUDA(cudaEventCreate(&e1));
+    const bool prof = g->prof.enabled;
+    g->prof.enabled = false;
+    float best = 0;
+    uint16_t pick = 0;
+    try {
+        for (uint16_t ch : cand) {
+            g->saba_choice = ch;
+            saba_run(g, depth, n_walks, c);  // warm-up (and the walk copy of this layout)
+            float t = 0;
+            for (int i = 0; i < std::max(trials, 1); ++i) {
+                TGTP_CUDA(cudaEventRecord(e0, g->stream));
+                saba_run(g, depth, n_walks, c);
+                TGTP_CUDA(cudaEventRecord(e1, g->stream));
+                TGTP_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                TGTP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                t = i == 0 ? ms : std::min(t, ms);
+            }
+            if (!pick || t < best) {
+                best = t;
+                pick = ch;
+            }
+        }
+    } catch (...) {
+        g->saba_choice = 0;
+        g->prof.enabled = prof;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    g->saba_choice = pick;
+    g->prof.enabled = prof;
+    TGTP_CUDA(cudaEventDestroy(e0));
+    TGTP_CUDA(cudaEventDestroy(e1));
+    return pick;
 }
 
 void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* host_sums3) {
