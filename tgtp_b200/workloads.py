@@ -9,7 +9,8 @@ Graphs: config1 (Chung-Lu n=4,039, 88,234 edges, exponent 2.5), config3 (R-MAT s
 factor 16, a=0.57), config4 (Chung-Lu n=10^6, 10^7 edges, exponent 2.3, seed 4), sparse5k
 (Chung-Lu n=5,000, 12,000 edges, exponent 2.1), sparse25k (Chung-Lu 28,000 ids, 120,000 edges,
 exponent 2.1, seed 1: largest component n=25,860, E=119,972), cl200k (Chung-Lu n=200,000, 2*10^6
-edges, exponent 2.3: a fifth of config4's scale), rmat16 (R-MAT scale 16, edge factor 16).  AESC inputs get 128 eigenpairs: from the scipy
+edges, exponent 2.3: a fifth of config4's scale), rmat16 (R-MAT scale 16, edge factor 16),
+batch_rmat (graph 28 of the batched workload: R-MAT, n=143,522, 1,732,704 edges, its eps 0.005).  AESC inputs get 128 eigenpairs: from the scipy
 eigen prep (written and parsed back as sorted_eigens_128.txt) up to 20,000 vertices, from the GPU
 eigen prep (tolerance 1e-4) above.  --deadline sets the device time budget of one kernel
 (TGTP_KERNEL_DEADLINE_S; default 30 s).  Prints one line per run: seconds and work counters.
@@ -37,6 +38,8 @@ def _graph(name: str):
         return synth.chung_lu(200_000, 2_000_000, 2.3, 4)
     if name == "rmat16":
         return synth.rmat(16, 16, 0.57, 0.19, 0.19, 2)
+    if name == "batch_rmat":
+        return synth.config5_graphs(5, 64)[28][0]
     if name == "config4":
         return synth.chung_lu(1_000_000, 10_000_000, 2.3, 4)
     raise SystemExit(f"unknown graph {name}")
