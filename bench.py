@@ -94,6 +94,7 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self._wait_for(1)  # a sample taken before the timed region starts
         except Exception:
             self.proc = None
         return self
@@ -102,8 +103,16 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def _wait_for(self, count, limit_s=5.0):
+        t0 = time.time()
+        while len(self.lines) < count and time.time() - t0 < limit_s:
+            time.sleep(0.01)
+
     def __exit__(self, *exc):
         if self.proc:
+            # the timed region can be shorter than the sampling period: keep sampling until one
+            # more sample has come in, so the region is bracketed by samples
+            self._wait_for(len(self.lines) + 1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)

@@ -88,6 +88,7 @@ def test_batch_replays_match_single_runs(manifest, cuda_device):
     for rep in range(2):
         for _, o in runs:
             o.fill_(-1.0)
+        torch.cuda.synchronize()  # the fills (torch's stream) end before the batch's stream
         b.run()
         b.wait()
         for (a, o), w, st in zip(runs, want, stats):
@@ -157,6 +158,7 @@ def test_one_persistent_launch_over_all_graphs_matches_single_runs(manifest, cud
         for rep in range(2):
             for _, o in runs:
                 o.fill_(-1.0)
+            torch.cuda.synchronize()  # the fills (torch's stream) end before the batch's stream
             b.run()
             b.wait()
             for (a, o), w, st in zip(runs, want, stats):

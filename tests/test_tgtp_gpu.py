@@ -248,3 +248,20 @@ def test_device_time_budget_gives_a_timeout_status_and_leaves_the_graph_usable(
         for k in STAT_KEYS:
             assert st[k] == want_st[k], k
     g.free()
+
+
+@pytest.mark.parametrize("name", ["cl300", "sparse400", "multi300"])
+def test_one_vertex_at_a_time_push_gives_the_same_bits(manifest, cuda_device, monkeypatch, name):
+    """The parity forms' push drains a window of frontier vertices per step by default; with
+    TGTP_GS_WINDOW=0 it drains one vertex at a time.  Both are the reference's sequential push:
+    the FP32 form equals the golden vectors either way."""
+    from tgtp_b200.aesc import AESC, AESCConfig
+
+    monkeypatch.setenv("TGTP_GS_WINDOW", "0")
+    c = golden_tgtp_case(manifest, name)
+    g = _device_graph(c)
+    for run in c["runs"]:
+        got = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"])).tgtp()
+        want = load_golden_scores(run)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), run
+    g.free()

@@ -971,6 +971,7 @@ struct SourceParams {
     // Vertex count the per-warp scratch is laid out for (the graph's n, or the largest n of a
     // batch whose graphs share the scratch of one persistent launch).
     uint32_t scratch_n;
+    bool gs_window;  // parity forms: the windowed sequential push (else one vertex at a time)
 };
 
 // The source kernel's parameters: one graph (N = 1), or up to N graphs whose listed rows one
@@ -1903,6 +1904,122 @@ source_kernel(Pack pk) {
                 pcost = 0;
                 st_pv += qs;
                 if constexpr (!JACOBI) {
+                if (p.gs_window) {
+                // ---- diffuse (:218-239), windowed ----
+                // The reference drains the frontier one vertex at a time: r = pvec[v], pvec[v] = 0,
+                // then pvec[u] += r / deg(u) for u in N(v) in row order, discovering each u on its
+                // first visit.  Here up to 32 consecutive frontier vertices form a window whose
+                // residuals are taken at once and whose rows are concatenated and processed 32
+                // entries per step, in order.  That gives the reference's values as long as no
+                // entry of a window vertex j targets a later window vertex k (it would have changed
+                // r_k before k was drained): such an entry cuts the window before k -- found before
+                // anything of its step is applied, the cut vertices get their residuals back and
+                // are drained by a later window.  Entries targeting the vertex itself or an earlier
+                // window vertex are ordinary adds (those were drained first in the reference too).
+                // Lanes of one step that hit the same neighbour form a group whose lowest lane adds
+                // the group's contributions one by one in lane (= the reference's) order; the
+                // lowest lane is also the first visit, so discovery order is the reference's.  vis
+                // holds 1 + the window index in its upper six bits while a vertex is in a window.
+                uint32_t* exs = reinterpret_cast<uint32_t*>(acc + 64 + 32);  // 33 entry offsets
+                uint32_t* vbs = exs + 33;                                     // 32 row starts
+                for (uint32_t i0 = 0; i0 < qs;) {
+                    const uint32_t cnt = min(32u, qs - i0);
+                    uint32_t myv = 0, vb = 0, vd = 0;
+                    Real rv = Real(0);
+                    if (lane < cnt) {
+                        myv = q[i0 + lane];
+                        vb = __ldg(idx + myv);
+                        vd = __ldg(idx + myv + 1) - vb;
+                        rv = pvec[myv];
+                    }
+                    __syncwarp();
+                    if (lane < cnt) {
+                        pvec[myv] = Real(0);
+                        vis[myv] = (unsigned char)((vis[myv] & 3u) | ((lane + 1u) << 2));
+                    }
+                    uint32_t incl = vd;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+                        if (lane >= uint32_t(o)) incl += y;
+                    }
+                    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+                    exs[lane] = incl - vd;
+                    vbs[lane] = vb;
+                    if (lane == 31) exs[32] = total;
+                    __syncwarp();
+                    uint32_t wend = cnt;  // the window: frontier vertices i0 .. i0 + wend - 1
+                    uint32_t pm = 0;      // entry cursor of the loader (one step ahead)
+                    auto load_step = [&](uint32_t e0, uint32_t& cur_m, uint32_t& sg, uint2& a) {
+                        const uint32_t e = e0 + lane;
+                        sg = 32u;
+                        a = make_uint2(NONE, 1u);
+                        if (e < total) {
+                            while (exs[cur_m + 1] <= e) ++cur_m;
+                            sg = cur_m;
+                            a = __ldg(p.adjd + vbs[cur_m] + (e - exs[cur_m]));
+                        }
+                    };
+                    uint32_t sg = 32u, nsg = 32u;
+                    uint2 ea, nea;
+                    load_step(0u, pm, sg, ea);
+                    for (uint32_t e0 = 0; e0 < total; e0 += 32) {
+                        if (e0 + 32 < total) load_step(e0 + 32, pm, nsg, nea);
+                        if (__all_sync(kFullMask, sg >= wend)) break;  // past the (cut) window
+                        const bool valid = sg < wend;
+                        const uint32_t u = ea.x, du = ea.y;
+                        const uint32_t vv = valid ? uint32_t(vis[u]) : 0u;
+                        const uint32_t wk = vv >> 2;  // 1 + window index of u, 0 if none
+                        const bool conflict = valid && wk > sg + 1u;
+                        if (__any_sync(kFullMask, conflict)) {
+                            uint32_t kmin = conflict ? wk - 1u : 32u;
+#pragma unroll
+                            for (int o = 16; o; o >>= 1) kmin = min(kmin, __shfl_xor_sync(kFullMask, kmin, o));
+                            // window vertices kmin .. wend - 1 leave the window undrained
+                            if (lane >= kmin && lane < wend) {
+                                pvec[myv] = rv;
+                                vis[myv] = (unsigned char)(vis[myv] & 3u);
+                            }
+                            wend = kmin;
+                            __syncwarp();
+                        }
+                        const bool apply = sg < wend;
+                        const uint32_t vis_u = apply ? uint32_t(vis[u]) : 0u;
+                        const unsigned grp = __match_any_sync(kFullMask, apply ? u : (0xffffffe0u | lane));
+                        const bool lead = apply && lane == uint32_t(__ffs(grp) - 1);
+                        const Real r = __shfl_sync(kFullMask, rv, int(sg & 31u));
+                        const Real c = apply ? rdiv(r, from_u64<Real>(du)) : Real(0);
+                        bool fresh = false;
+                        if (lead && (vis_u & 1u) == 0u) {
+                            vis[u] = (unsigned char)(vis_u | 1u);
+                            fresh = true;
+                        }
+                        const unsigned bal = __ballot_sync(kFullMask, fresh);
+                        if (fresh) {
+                            qn[qns + __popc(bal & lt)] = u;
+                            pcost += du;
+                        }
+                        qns += __popc(bal);
+                        const unsigned others = __ballot_sync(kFullMask, apply && !lead);
+                        Real pv = Real(0);
+                        if (lead) pv = radd(pvec[u], c);
+                        for (unsigned mm = others; mm; mm &= mm - 1) {
+                            const int t = __ffs(mm) - 1;
+                            const Real ct = __shfl_sync(kFullMask, c, t);
+                            if (lead && ((grp >> t) & 1u)) pv = radd(pv, ct);
+                        }
+                        if (lead) pvec[u] = pv;
+                        __syncwarp();
+                        sg = nsg;
+                        ea = nea;
+                        nsg = 32u;
+                    }
+                    if (lane < wend) vis[myv] = (unsigned char)(vis[myv] & 3u);
+                    st_tr += __shfl_sync(kFullMask, incl, int(wend - 1));
+                    __syncwarp();
+                    i0 += wend;
+                }
+                } else {
                 // ---- diffuse (:218-239) ----
                 // The frontier is drained in order, one vertex at a time; the lanes share the
                 // vertex's adjacency (distinct neighbours, so the lanes' flag and residual updates
@@ -2005,6 +2122,7 @@ source_kernel(Pack pk) {
                             cco[jj] = nc[jj];
                         }
                     }
+                }
                 }
                 } else {
                     // ---- Jacobi push (mixed form) ----
@@ -3041,6 +3159,10 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.pre_final = nullptr;
     p.multi = multi;
     p.scratch_n = uint32_t(n);
+    {
+        const char* e = std::getenv("TGTP_GS_WINDOW");  // "0": one frontier vertex at a time
+        p.gs_window = !(e && std::string(e) == "0");
+    }
     Pack1 pk;
     pk.count = 1;
     if (!block_mode) {

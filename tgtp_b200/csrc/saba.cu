@@ -433,14 +433,17 @@ void saba_prepare(tgtp_graph* g) {
 }
 
 // Whether saba_count walks the inlined copy (one dependent 16-byte load per hop) or the plain
-// renumbered copy (two): TGTP_SABA_INLINE=0/1 decides, else the inlined copy is used while its
-// 16 bytes per slot stay within 2 GiB.
+// renumbered copy (two): the tuned choice (saba_tune), else TGTP_SABA_INLINE=0/1, else the inlined
+// copy while its 16 bytes per slot stay within 48 MB.  Walks are random, so the copies are read
+// from L2: on the 4,039-vertex graph (2.8 MB inlined) the inlined copy measured 1.5x the plain
+// one; on R-MAT scale 18 (122 MB inlined against 33 MB plain, beside a 126 MB L2) it measured
+// 0.8x, the inlined copy no longer fitting.  saba_tune may still try it up to 2 GiB.
 bool saba_inline_fits(const tgtp_graph* g) { return g->m * sizeof(uint4) <= (size_t(2) << 30); }
 
 bool saba_use_inline(const tgtp_graph* g) {
     if (g->saba_choice) return (g->saba_choice & 0x100) != 0;
     if (const char* e = std::getenv("TGTP_SABA_INLINE")) return std::atoi(e) != 0;
-    return saba_inline_fits(g);
+    return g->m * sizeof(uint4) <= size_t(48) << 20;
 }
 
 void saba_prepare_inline(tgtp_graph* g) {
