@@ -152,6 +152,9 @@ tgtp_status tgtp_batch_create(tgtp_graph* const* graphs, const tgtp_config* conf
             aesc_read_stats(graphs[i], st);  // measures which push suits a mixed run
             if (tune_trials <= 0) aesc_run(graphs[i], configs[i], device_scores[i]);
         }
+        // The replays run on the CUDA graph's own streams, which do not wait for work still
+        // queued on the handles' streams: let those plain runs finish before the first replay.
+        for (uint32_t i = 0; i < count; ++i) aesc_check_flags(graphs[i]);
         auto b = std::make_unique<tgtp_batch>();
         b->origin = stream_acquire();
         for (uint32_t i = 0; i < count; ++i) {
