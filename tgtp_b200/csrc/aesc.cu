@@ -1261,6 +1261,7 @@ push_block_kernel(PushBlockParams p) {
     __shared__ int s_any;
     __shared__ uint32_t s_tmp[32];
     __shared__ uint32_t s_lc, s_lp, s_ln, s_pn;  // list lengths
+    __shared__ uint32_t s_next;                  // next row of the round (claimed by warps)
     __shared__ unsigned long long s_live_deg;   // degree sum of the running-live rows of cur
     pdl_launch_dependents();
     pdl_wait();  // the list, and the previous wave's readers of these blocks
@@ -1434,6 +1435,7 @@ push_block_kernel(PushBlockParams p) {
         if (threadIdx.x == 0) {
             s_ln = 0;
             s_live_deg = 0;
+            s_next = nwarp;
         }
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
         __syncthreads();
@@ -1442,7 +1444,9 @@ push_block_kernel(PushBlockParams p) {
         unsigned long long pc = 0, live_deg = 0;
         uint32_t sup = 0;
         float mx = 0.f, mn = 1.f;
-        for (uint32_t k = warp; k < nrows; k += nwarp) {
+        // rows are claimed one at a time from a shared counter (row k = warp first), so a warp
+        // that meets a hub row does not hold the others at the round's barrier
+        for (uint32_t k = warp; k < nrows;) {
             const uint32_t u = compact ? P[k] : k;
             const uint32_t ub = __ldg(p.idx + u), ud = __ldg(p.idx + u + 1) - ub;
             unsigned long long acc = 0;
@@ -1459,6 +1463,15 @@ push_block_kernel(PushBlockParams p) {
                 const uint32_t packed = __shfl_sync(kFullMask, nb, nth);
                 const uint32_t kk = __popc(live);
                 uint32_t t = 0;
+                // eight independent 128-byte row loads in flight per step
+                for (; t + 8 <= kk; t += 8) {
+                    float x[8];
+#pragma unroll
+                    for (int h = 0; h < 8; ++h)
+                        x[h] = cur[size_t(__shfl_sync(kFullMask, packed, t + h)) * S + lane];
+#pragma unroll
+                    for (int h = 0; h < 8; ++h) acc += to_fixed(x[h]);
+                }
                 for (; t + 4 <= kk; t += 4) {
                     const float x0 = cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane];
                     const float x1 = cur[size_t(__shfl_sync(kFullMask, packed, t + 1)) * S + lane];
@@ -1489,6 +1502,9 @@ push_block_kernel(PushBlockParams p) {
                 if (any_nz) Ln[atomicAdd(&s_ln, 1u)] = u;
             }
             nxt[size_t(u) * S + lane] = r;
+            unsigned nk = 0;
+            if (lane == 0) nk = atomicAdd(&s_next, 1u);
+            k = __shfl_sync(kFullMask, nk, 0);
         }
         if (run) {
             atomicAdd(s_picost + lane, pc);
@@ -1776,15 +1792,26 @@ source_kernel(Pack pk) {
                               size_t(col) * n;
             if constexpr (!SMEM && std::is_same<Real, float>::value) pvec = const_cast<Real*>(cb);
             uint32_t cq = 0;
-            for (uint32_t i0 = 0; i0 < n; i0 += 32) {
-                const uint32_t i = i0 + lane;
-                const Real x = i < n ? Real(cb[i]) : Real(0);
-                if (SMEM && i < n) pvec[i] = x;
-                const bool nz = x > Real(0);
-                const unsigned bal = __ballot_sync(kFullMask, nz);
-                if (nz) q[cq + __popc(bal & lt)] = i;
-                cq += __popc(bal);
-            }
+            // the scan keeps 2 x kB coalesced 128-byte loads in flight (pipelined)
+            pipelined<Real>(n,
+                [&](uint32_t i0, Real* r) {
+#pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        const uint32_t i = i0 + 32 * b + lane;
+                        r[b] = i < n ? Real(cb[i]) : Real(0);
+                    }
+                },
+                [&](uint32_t i0, const Real* r) {
+#pragma unroll
+                    for (int b = 0; b < kB; ++b) {
+                        const uint32_t i = i0 + 32 * b + lane;
+                        if (SMEM && i < n) pvec[i] = r[b];
+                        const bool nz = r[b] > Real(0);
+                        const unsigned bal = __ballot_sync(kFullMask, nz);
+                        if (nz) q[cq + __popc(bal & lt)] = i;
+                        cq += __popc(bal);
+                    }
+                });
             __syncwarp();
             qs = cq;
             ell = pr.ell;
