@@ -155,7 +155,9 @@ tgtp_status tgtp_last_taus(tgtp_graph* g, int32_t* host_taus);
  * under every layout.  *layout (may be NULL) receives the choice: 0x100 bit = shared memory, low
  * byte = warps per block, 0x200 = block push, bits 12-13 = its compaction threshold (a round is
  * compacted to the rows next to the live ones when their degree sum is below m / 4, m / 2,
- * m / 16, or never).  The reference has no counterpart (its OpenMP loop has one layout). */
+ * m / 16, or never); for the FP32 and FP64 forms 0x400 = the windowed sequential push, 0x800 =
+ * one frontier vertex at a time.  The reference has no counterpart (its OpenMP loop has one
+ * layout). */
 tgtp_status tgtp_graph_tune(tgtp_graph* g, const tgtp_config* cfg, float* device_scores,
                             int32_t trials, int32_t* layout);
 

@@ -265,3 +265,25 @@ def test_one_vertex_at_a_time_push_gives_the_same_bits(manifest, cuda_device, mo
         want = load_golden_scores(run)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), run
     g.free()
+
+
+@pytest.mark.parametrize("window", ["0", "1"])
+def test_config1_both_sequential_pushes_are_bit_exact(cuda_device, oracle_lib, config1_inputs,
+                                                      monkeypatch, window):
+    """On the 4,039-vertex graph (44 entries per row: the default drains one frontier vertex at a
+    time) both the windowed and the one-vertex push give the oracle's FP32 and FP64 bits at
+    eps = 0.005, where sources push for several rounds."""
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, PRECISION_FP64, VEC_F32, VEC_F64
+
+    monkeypatch.setenv("TGTP_GS_WINDOW", window)
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    got32 = AESC(g, AESCConfig(0.005)).tgtp()
+    got64 = AESC(g, AESCConfig(0.005, precision=PRECISION_FP64)).tgtp()
+    g.free()
+    want32 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v32"], 0.005)
+    want64 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], 0.005, fp64=True)
+    assert np.array_equal(got32.view(np.uint32), want32.view(np.uint32))
+    assert np.array_equal(got64.view(np.uint32), want64.view(np.uint32))

@@ -76,6 +76,10 @@ static_assert(kStCount <= kRunStatSlots, "aesc_read_stats writes kStCount counte
 // warps per block; 0 = the default rule.
 constexpr uint16_t kLayoutSmem = 0x100;
 constexpr uint16_t kLayoutBlock = 0x200;  // mixed form: multi-source block push
+// parity forms: bit 0x400 set = the windowed sequential push, 0x800 = one vertex at a time (neither
+// set: the default rule, by average degree)
+constexpr uint16_t kLayoutWindow = 0x400;
+constexpr uint16_t kLayoutNoWindow = 0x800;
 // block push: the frontier size below which a round is compacted, as m / list_div, in bits 12-13
 // (0 = the default list_div of 4, 1 = 2, 2 = 16, 3 = never compacted)
 constexpr int kLayoutListShift = 12;
@@ -3187,8 +3191,18 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.multi = multi;
     p.scratch_n = uint32_t(n);
     {
-        const char* e = std::getenv("TGTP_GS_WINDOW");  // "0": one frontier vertex at a time
-        p.gs_window = !(e && std::string(e) == "0");
+        // The windowed push pays off when rows are short: several frontier vertices share a
+        // 32-entry step.  When rows average 32 entries or more, each vertex fills its steps anyway
+        // and adjacent frontier vertices cut windows often, so one vertex at a time is used
+        // (4,039-vertex Chung-Lu graph, 44 entries per row: 0.73 against 0.86 ms at eps = 0.01;
+        // sparse Chung-Lu, 9.3 per row: 4.1 against 1.4 s at eps = 0.005).  The tuned layout,
+        // then TGTP_GS_WINDOW=0/1, override the rule.
+        const uint16_t lay = g->src_layout[key];
+        const char* e = std::getenv("TGTP_GS_WINDOW");
+        if (lay & kLayoutWindow) p.gs_window = true;
+        else if (lay & kLayoutNoWindow) p.gs_window = false;
+        else if (e) p.gs_window = std::string(e) != "0";
+        else p.gs_window = m < 32 * n;
     }
     Pack1 pk;
     pk.count = 1;
@@ -3513,9 +3527,14 @@ int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int t
     size_t per_warp = ((g->n * rs + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
     if (mixed && per_warp + 8 * g->n <= size_t(112) * 1024) per_warp += 8 * g->n;
     std::vector<uint16_t> cand;
-    for (int w : {1, 2})
-        if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(kLayoutSmem | w));
-    for (int w : {1, 2, 4}) cand.push_back(uint16_t(w));
+    // the parity forms also try the windowed and the one-vertex-at-a-time push in each layout
+    const std::vector<uint16_t> push_kinds =
+        mixed ? std::vector<uint16_t>{0} : std::vector<uint16_t>{kLayoutWindow, kLayoutNoWindow};
+    for (uint16_t pk : push_kinds) {
+        for (int w : {1, 2})
+            if (per_warp * w <= size_t(227) * 1024) cand.push_back(uint16_t(pk | kLayoutSmem | w));
+        for (int w : {1, 2, 4}) cand.push_back(uint16_t(pk | w));
+    }
     if (mixed) {  // the block push, with the per-source stage in the best layout that fits,
                   // at each compaction threshold
         const uint16_t post = per_warp <= size_t(112) * 1024 ? uint16_t(kLayoutSmem | 1) : uint16_t(4);
