@@ -1134,6 +1134,88 @@ __device__ void kth_largest(const uint32_t* q, uint32_t qs, const Real* pvec, in
     }
 }
 
+// kth_largest over the positive entries of a dense vector (the residual column the block push
+// leaves, whose positive entries are exactly the final frontier, in vertex order): the same
+// selection without the frontier list, as contiguous pipelined loads.
+template <class Real>
+__device__ void kth_largest_col(const Real* col, uint32_t n, int rg, Real& t, int& n_eq_taken) {
+    const uint32_t lane = threadIdx.x & 31;
+    auto load_v = [&](uint32_t i0, Real* r) {
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+            const uint32_t i = i0 + 32 * b + lane;
+            const Real x = i < n ? col[i] : Real(0);
+            r[b] = x > Real(0) ? x : Real(-INFINITY);
+        }
+    };
+    if (rg <= kTopK) {
+        Real L[kTopK];
+#pragma unroll
+        for (int j = 0; j < kTopK; ++j) L[j] = Real(-INFINITY);
+        pipelined<Real>(n, load_v, [&](uint32_t, const Real* r) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                const Real x = r[b];
+                if (x > L[kTopK - 1]) {
+#pragma unroll
+                    for (int j = kTopK - 1; j > 0; --j) {
+                        const Real prev = L[j - 1];
+                        L[j] = x > prev ? prev : (x > L[j] ? x : L[j]);
+                    }
+                    L[0] = x > L[0] ? x : L[0];
+                }
+            }
+        });
+        Real last = Real(-INFINITY);
+        int run = 0;
+        for (int r = 0; r < rg; ++r) {
+            const Real mx = warp_max(L[0]);
+            const unsigned who = __ballot_sync(kFullMask, L[0] == mx);
+            if (lane == uint32_t(__ffs(who) - 1)) {
+#pragma unroll
+                for (int j = 0; j < kTopK - 1; ++j) L[j] = L[j + 1];
+                L[kTopK - 1] = Real(-INFINITY);
+            }
+            run = (r > 0 && mx == last) ? run + 1 : 1;
+            last = mx;
+        }
+        t = last;
+        n_eq_taken = run;
+        return;
+    }
+    Real thr = Real(INFINITY);
+    int remaining = rg;
+    while (true) {
+        Real best = Real(-INFINITY);
+        unsigned cnt = 0;
+        pipelined<Real>(n, load_v, [&](uint32_t, const Real* r) {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) {
+                const Real x = r[b];
+                if (x < thr && x > Real(-INFINITY)) {
+                    if (x > best) {
+                        best = x;
+                        cnt = 1;
+                    } else if (x == best) {
+                        ++cnt;
+                    }
+                }
+            }
+        });
+        const Real mx = warp_max(best);
+        unsigned c = best == mx ? cnt : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(kFullMask, c, o);
+        if (int(c) >= remaining) {
+            t = mx;
+            n_eq_taken = remaining;
+            return;
+        }
+        remaining -= int(c);
+        thr = mx;
+    }
+}
+
 // Segmented max / min over lanes whose segment ids are non-decreasing: after the shuffles, the
 // last lane of each segment holds the segment's extremum.
 template <class Real>
@@ -1796,8 +1878,12 @@ source_kernel(Pack pk) {
                               size_t(col) * n;
             if constexpr (!SMEM && std::is_same<Real, float>::value) pvec = const_cast<Real*>(cb);
             uint32_t cq = 0;
-            // the scan keeps 2 x kB coalesced 128-byte loads in flight (pipelined)
-            pipelined<Real>(n,
+            // HBM tier: the column is read in place and the edge bound selects from it directly
+            // (its positive entries are the frontier, in vertex order), so no frontier list is
+            // built; the shared-memory tier copies the column and lists the frontier.  The scan
+            // keeps 2 x kB coalesced 128-byte loads in flight (pipelined).
+            if (!SMEM) cq = pr.support;
+            else pipelined<Real>(n,
                 [&](uint32_t i0, Real* r) {
 #pragma unroll
                     for (int b = 0; b < kB; ++b) {
@@ -2371,7 +2457,58 @@ source_kernel(Pack pk) {
             uint32_t* set = qn;  // free after the last swap
             int sc = 0;
             Real gamma_max;
-            if (p.gamma < nnz) {
+            const bool from_col = !SMEM && p.pre != nullptr;  // select from the column
+            if (p.gamma < nnz && from_col) {
+                Real t;
+                int need_eq;
+                kth_largest_col<Real>(pvec, n, rg, t, need_eq);
+                int taken_eq = 0;
+                pipelined<Real>(n,
+                    [&](uint32_t i0, Real* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            r[b] = i < n ? pvec[i] : Real(0);
+                        }
+                    },
+                    [&](uint32_t i0, const Real* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            const Real x = r[b] > Real(0) ? r[b] : Real(-INFINITY);
+                            const bool gt = x > t, eq = x == t;
+                            const unsigned be = __ballot_sync(kFullMask, eq);
+                            const bool take_eq = eq && taken_eq + __popc(be & lt) < need_eq;
+                            const bool take = (gt || take_eq) && sc < rg;
+                            const unsigned bt = __ballot_sync(kFullMask, take);
+                            if (take) set[sc + __popc(bt & lt)] = i;
+                            sc += __popc(bt);
+                            taken_eq += __popc(__ballot_sync(kFullMask, take_eq));
+                        }
+                    });
+                gamma_max = std_min(Real(1), t);
+            } else if (from_col) {
+                // every frontier vertex is in the set: the column's positive entries in order
+                pipelined<Real>(n,
+                    [&](uint32_t i0, Real* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            r[b] = i < n ? pvec[i] : Real(0);
+                        }
+                    },
+                    [&](uint32_t i0, const Real* r) {
+#pragma unroll
+                        for (int b = 0; b < kB; ++b) {
+                            const uint32_t i = i0 + 32 * b + lane;
+                            const bool nz = r[b] > Real(0);
+                            const unsigned bal = __ballot_sync(kFullMask, nz);
+                            if (nz) set[sc + __popc(bal & lt)] = i;
+                            sc += __popc(bal);
+                        }
+                    });
+                gamma_max = Real(0);
+            } else if (p.gamma < nnz) {
                 Real t;
                 int need_eq;
                 kth_largest<Real>(q, qs, pvec, rg, t, need_eq);
