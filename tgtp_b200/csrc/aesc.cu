@@ -1688,11 +1688,12 @@ __global__ void row_key_kernel(const uint32_t* __restrict__ idx, const int* __re
     }
 }
 
-// The mixed form's HBM-tier variant keeps at least three 128-thread blocks per SM (at most 168
-// registers, as it compiled before its column edge bound was added): after the block push its
-// phases are latency-bound on HBM and need the warps.
+// The HBM-tier variants with FP32 residuals keep at least three 128-thread blocks per SM (at most
+// 168 registers, the occupancy they had before the windowed push and the column edge bound were
+// added): their phases are latency-bound on HBM and need the warps.  The FP64 variant compiled to
+// about 240 registers (two blocks per SM) without spills before and is left so.
 template <class Real, class Acc, bool SMEM, bool JACOBI, class Pack>
-__global__ void __launch_bounds__(kSrcMaxThreads, (!SMEM && JACOBI) ? 3 : 1)
+__global__ void __launch_bounds__(kSrcMaxThreads, (!SMEM && sizeof(Real) == 4) ? 3 : 1)
 source_kernel(Pack pk) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_pre[Pack::kMax + 1];  // item prefix over the pack's row lists
