@@ -124,3 +124,30 @@ def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, ctas,
             assert np.array_equal(got["0"][1], got["1"][1])
             assert got["0"][2] == got["1"][2], (run, got["0"][2], got["1"][2])
     g.free()
+
+
+@pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
+def test_mixed_block_push_with_hbm_per_source_stage_gives_the_same_bits(manifest, cuda_device,
+                                                                         name, monkeypatch):
+    """After the block push, the per-source stage in the HBM tier reads each source's residual
+    column in place and selects the top-gamma residuals straight from it (no frontier list), as
+    on large graphs; its scores, taus and counters equal the per-warp push's."""
+    from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_MIXED, VEC_BF16
+
+    monkeypatch.setenv("TGTP_PVEC_TIER", "global")
+    monkeypatch.setenv("TGTP_BLOCK_CTAS", "2")
+    c = golden_tgtp_case(manifest, name)
+    g = _graph(c)
+    for run in c["runs"]:
+        got = {}
+        for block in ("0", "1"):
+            monkeypatch.setenv("TGTP_MIXED_BLOCK", block)
+            a = AESC(g, AESCConfig(run["epsilon"], omega=c["omega"], gamma=run["gamma"],
+                                   precision=PRECISION_MIXED, vec_dtype=VEC_BF16))
+            s = a.tgtp()
+            st = a.stats()
+            got[block] = (s, {k: st[k] for k in ("push_rounds", "walk_edges", "walk_count",
+                                                 "walk_hops")})
+        assert np.array_equal(got["0"][0].view(np.uint32), got["1"][0].view(np.uint32)), run
+        assert got["0"][1] == got["1"][1], run
+    g.free()
