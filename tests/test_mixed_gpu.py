@@ -87,7 +87,8 @@ def test_mixed_matches_fp64_when_no_walks_run(cuda_device, config1_inputs):
     g.free()
 
 
-@pytest.mark.parametrize("rounds", ["auto", "compact", "full", "compact_global_masks"])
+@pytest.mark.parametrize("rounds", ["auto", "compact", "full", "compact_global_masks",
+                                    "compact_cur_masks"])
 @pytest.mark.parametrize("ctas", ["0", "2"])
 @pytest.mark.parametrize("name", ["cl300", "sparse400", "grid", "cycle9", "complete12"])
 def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, ctas, rounds,
@@ -96,14 +97,17 @@ def test_mixed_block_push_gives_the_same_bits(manifest, cuda_device, name, ctas,
     give identical scores, taus and work counters.  ctas = 2 runs the block push with two CTAs,
     64 sources per wave, so the larger graphs take several waves.  The block push's rounds are
     chosen by their frontier size (auto), or all compacted to the rows next to the live ones, or
-    all full passes; compact_global_masks keeps its row masks in global memory, as on graphs whose
-    masks do not fit in shared memory."""
+    all full passes; compact_global_masks keeps its row masks in global memory and
+    compact_cur_masks only the current round's mask in shared memory, as on graphs whose masks do
+    not all fit in shared memory."""
     if ctas != "0":
         monkeypatch.setenv("TGTP_BLOCK_CTAS", ctas)
     if rounds != "auto":
         monkeypatch.setenv("TGTP_BLOCK_ROUNDS", rounds.split("_")[0])
     if rounds == "compact_global_masks":
         monkeypatch.setenv("TGTP_BLOCK_MASKS", "global")
+    if rounds == "compact_cur_masks":  # only the current round's mask in shared memory
+        monkeypatch.setenv("TGTP_BLOCK_MASKS", "cur")
     from tgtp_b200.aesc import AESC, AESCConfig, PRECISION_MIXED, VEC_BF16, VEC_F32
 
     c = golden_tgtp_case(manifest, name)

@@ -1266,6 +1266,7 @@ struct PushBlockParams {
     uint32_t* final_buf;   // per CTA: the block that holds the final columns
     PrePush* pre;          // per list entry
     bool bits;             // the three row masks fit in shared memory (else they live in gbits)
+    bool cur_smem;         // (when !bits) the current round's mask alone fits in shared memory
     uint32_t* gbits;       // per CTA: three n-bit row masks in global memory (L2), when not in smem
     uint32_t* lists;       // per CTA: four row lists of n entries (see push_block_kernel)
     uint32_t list_div;     // a round is compacted when its live rows' degree sum * list_div < m
@@ -1366,11 +1367,18 @@ push_block_kernel(PushBlockParams p) {
     for (size_t i = threadIdx.x; i < size_t(n) * S / 2; i += blockDim.x)
         reinterpret_cast<float4*>(A)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t words = (n + 31) / 32;
-    uint32_t* const bits_base = p.bits ? s_bits : p.gbits + size_t(blockIdx.x) * 3 * words;
-    uint32_t* bcur = bits_base;
-    uint32_t* bnxt = bits_base + words;
-    uint32_t* tmask = bits_base + 2 * words;
-    for (uint32_t i = threadIdx.x; i < 3 * words; i += blockDim.x) bits_base[i] = 0u;
+    // Mask placement: all three in shared memory; or (cur_smem) bcur in shared memory -- it is
+    // read for every neighbour chunk of the pull -- with bnxt and tmask in global memory, bnxt
+    // copied into bcur at each round's end; or all three in global memory.
+    uint32_t* const gb = p.gbits ? p.gbits + size_t(blockIdx.x) * 3 * words : nullptr;
+    uint32_t* bcur = (p.bits || p.cur_smem) ? s_bits : gb;
+    uint32_t* bnxt = p.bits ? s_bits + words : gb + words;
+    uint32_t* tmask = p.bits ? s_bits + 2 * words : gb + 2 * words;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        bcur[i] = 0u;
+        bnxt[i] = 0u;
+        tmask[i] = 0u;
+    }
     uint32_t* const lbase = p.lists + size_t(blockIdx.x) * 4 * size_t(n);
     uint32_t* Lc = lbase;
     uint32_t* Lp = lbase + n;
@@ -1620,9 +1628,15 @@ push_block_kernel(PushBlockParams p) {
         float* t = cur;
         cur = nxt;
         nxt = t;
-        uint32_t* tb = bcur;
-        bcur = bnxt;
-        bnxt = tb;
+        if (!p.bits && p.cur_smem) {
+            // bcur stays in shared memory: take the new round's mask into it
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bcur[i] = bnxt[i];
+            __syncthreads();
+        } else {
+            uint32_t* tb = bcur;
+            bcur = bnxt;
+            bnxt = tb;
+        }
         uint32_t* tl = Lp;
         Lp = Lc;
         Lc = Ln;
@@ -3377,14 +3391,22 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         bp.pre = g->block_pre.as<PrePush>();
         bp.stats = stats;
         bp.budget_ns = p.budget_ns;
-        // two row bitmasks in shared memory while they fit beside the kernel's static 1.3 KB
-        // three row masks in shared memory while they fit beside the kernel's static 1.5 KB,
-        // else in global memory; four row lists of n entries per CTA
-        const size_t bits_bytes = 3 * sizeof(uint32_t) * ((size_t(n) + 31) / 32);
+        // three row masks in shared memory while they fit beside the kernel's static 1.5 KB, else
+        // the current round's mask alone (n up to about 1.6 million), else none; the others in
+        // global memory; four row lists of n entries per CTA.  TGTP_BLOCK_MASKS=global|cur picks
+        // the placement of larger graphs on small ones.
+        const size_t mask_bytes = sizeof(uint32_t) * ((size_t(n) + 31) / 32);
+        const size_t bits_bytes = 3 * mask_bytes;
         bp.bits = bits_bytes <= size_t(200) * 1024;
-        if (const char* e = std::getenv("TGTP_BLOCK_MASKS"))  // "global": as for large graphs
-            if (std::string(e) == "global") bp.bits = false;
-        const size_t bsm = bp.bits ? bits_bytes : 0;
+        bp.cur_smem = !bp.bits && mask_bytes <= size_t(200) * 1024;
+        if (const char* e = std::getenv("TGTP_BLOCK_MASKS")) {
+            if (std::string(e) == "global") bp.bits = bp.cur_smem = false;
+            else if (std::string(e) == "cur") {
+                bp.bits = false;
+                bp.cur_smem = true;
+            }
+        }
+        const size_t bsm = bp.bits ? bits_bytes : (bp.cur_smem ? mask_bytes : 0);
         if (!bp.bits) grow(g, g->block_bits, bits_bytes * block_ctas + 16);
         bp.gbits = bp.bits ? nullptr : g->block_bits.as<uint32_t>();
         grow(g, g->block_lists, sizeof(uint32_t) * 4 * size_t(n) * block_ctas + 16);
