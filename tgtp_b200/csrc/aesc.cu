@@ -2736,6 +2736,12 @@ source_kernel(Pack pk) {
             unsigned long long bi = 0;
             uint32_t len = 0, step = 0, cur = 0, cur2 = 0, sec = 0, sec2 = 0, state = 0;
             Real x = Real(0);
+            // Each hop's residual difference is added to x one hop later (after the next hop's
+            // row offsets are requested), so the residual loads overlap the next hop instead of
+            // stalling it; the adds stay in hop order, and the last one is made before the
+            // item's lanes are summed.
+            Real pa = Real(0), pb = Real(0);
+            bool pend = false;
             while (true) {
                 const unsigned need = __ballot_sync(kFullMask, !has && j == 0);
                 if (!has) {
@@ -2774,6 +2780,7 @@ source_kernel(Pack pk) {
                 if (has) {
                     const uint32_t b1 = __ldg(idx + cur), d1 = __ldg(idx + cur + 1) - b1;
                     const uint32_t b2 = __ldg(idx + cur2), d2 = __ldg(idx + cur2 + 1) - b2;
+                    if (pend) x = radd(x, rsub(pa, pb));
                     uint32_t k1, k2;
                     if (primary) {
                         k1 = __umulhi(sec ^ fmix32(cur), d1);
@@ -2788,7 +2795,9 @@ source_kernel(Pack pk) {
                     }
                     cur = __ldg(adj + b1 + k1);
                     cur2 = __ldg(adj + b2 + k2);
-                    x = radd(x, rsub(pvec[cur], pvec[cur2]));
+                    pa = pvec[cur];
+                    pb = pvec[cur2];
+                    pend = true;
                     if (++len == it.len) {
                         bi += 8;
                         start = true;
@@ -2796,6 +2805,10 @@ source_kernel(Pack pk) {
                     }
                 }
                 if (__any_sync(kFullMask, item_done)) {
+                    if (item_done && pend) {
+                        x = radd(x, rsub(pa, pb));
+                        pend = false;
+                    }
                     if constexpr (std::is_same<Real, Acc>::value) {
                         // the eight lanes summed 0..7, then preds += xij / (ds * nr) (:386-390, :525)
                         Real s = Real(0);
