@@ -219,30 +219,46 @@ def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3):
 
 def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
     """SABA walk counter at scale: seeded R-MAT scale 18, edge factor 16 (a=0.57, b=c=0.19), largest
-    component; depth 5, 2048 walks per vertex.  Kernel time from the library's CUDA events (3 runs
-    after 1 warm-up); transitions = active vertices x walks x depth; 20 algorithmic bytes per
-    transition (idx pair 8, adj 4, counter read + write 8).  The reference's rw_experiment_saba,
-    built from its sources, timed once on the host cores beside it."""
+    component; depth 5, 2048 walks per vertex, and beside it every depth x walks cell of the
+    walk experiment (D 5 / 10 / 15 x W 2,048 / 16,384).  Kernel time from the library's CUDA events
+    (3 runs after 1 warm-up); transitions = active vertices x walks x depth; 20 algorithmic bytes
+    per transition (idx pair 8, adj 4, counter read + write 8).  The reference's
+    rw_experiment_saba, built from its sources, timed once on the host cores beside it (D 5,
+    W 2,048)."""
     from tgtp_b200 import synth
     from tgtp_b200.aesc import AESCGraph, saba_count
 
     g = synth.config3_graph(1)
     idx, adj = g.csr()
     dg = AESCGraph.from_csr(idx, adj)
-    saba_count(dg, 5, 2048, counters=False)
-    dg.set_profiling(True)
-    for _ in range(3):
-        _, vc, cs, fb = saba_count(dg, 5, 2048, counters=False)
-    ks = dg.kernel_stats()
-    dg.set_profiling(False)
-    dg.free()
-    ms = ks["saba_walk"][1] / ks["saba_walk"][0]
-    trans = g.n * 2048 * 5
+
+    def cell(depth, walks):
+        saba_count(dg, depth, walks, counters=False)
+        dg.set_profiling(True)
+        for _ in range(3):
+            _, vc, cs, fb = saba_count(dg, depth, walks, counters=False)
+        ks = dg.kernel_stats()
+        dg.set_profiling(False)
+        ms = ks["saba_walk"][1] / ks["saba_walk"][0]
+        trans = g.n * walks * depth
+        return ms, ks, trans, vc, cs, fb
+
+    ms, ks, trans, vc, cs, fb = cell(5, 2048)
     out = {"workload": f"SABA d5 w2048 on R-MAT scale 18 (LCC n={g.n}, E={g.num_edges})",
            "transitions_per_s": trans / (ms * 1e-3), "kernel_ms": ms,
            "kernel_ms_all": {k: v[1] / v[0] for k, v in ks.items()},
            "hbm_frac_of_" + peak_kind: trans * 20 / (ms * 1e-3) / 1e9 / hbm,
            "visit_count": vc, "checksum": cs, "fallback_bouquets": fb}
+    cells = []
+    for depth in (5, 10, 15):
+        for walks in (2048, 16384):
+            ms_c, _, tr_c, vc_c, cs_c, _ = cell(depth, walks)
+            cells.append({"depth": depth, "walks": walks, "kernel_ms": ms_c,
+                          "transitions_per_s": tr_c / (ms_c * 1e-3),
+                          "hbm_frac_of_" + peak_kind: tr_c * 20 / (ms_c * 1e-3) / 1e9 / hbm,
+                          "visit_count": vc_c, "checksum": cs_c})
+    out["cells"] = cells
+    dg.free()
     if with_cpu:
         ref = saba_cpu_reference(g, root, 5, 2048)
         if ref is not None:

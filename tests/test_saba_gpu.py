@@ -176,8 +176,9 @@ def test_saba_rmat18_static_entry_point_matches_the_fixture(cuda_device, rmat18,
 
 
 def test_saba_tuned_layout_gives_the_same_counters(cuda_device, oracle_lib):
-    """saba_tune times 1 / 2 / 4 walkers per lane over the plain and the inlined walk copy and
-    keeps the fastest; every layout, and so the chosen one, gives the oracle's counters."""
+    """saba_tune times 1 / 2 / 4 walkers per lane over the plain walk copy (with 0 / 2,048 / 4,096
+    row records in shared memory) and the inlined one and keeps the fastest; every layout, and so
+    the chosen one, gives the oracle's counters."""
     from tgtp_b200 import synth
     from tgtp_b200.aesc import AESCGraph, saba_count, saba_tune
 
@@ -186,7 +187,8 @@ def test_saba_tuned_layout_gives_the_same_counters(cuda_device, oracle_lib):
     want = oracle_lib.saba(idx, adj, 7, 32)
     dg = AESCGraph.from_csr(idx, adj)
     choice = saba_tune(dg, 7, 32, trials=1)
-    assert (choice & 0xff) in (1, 2, 4) and (choice & ~0x1ff) == 0
+    assert (choice & 0xff) in (1, 2, 4) and (choice & ~0x71ff) == 0
+    assert (choice >> 12) in (0, 2, 3) and not ((choice & 0x100) and (choice >> 12))
     counts, visits, _, _ = saba_count(dg, 7, 32)
     assert np.array_equal(counts.astype(np.uint64), want)
     assert visits == g.n * 32 * 7
@@ -208,4 +210,29 @@ def test_saba_every_walk_layout_matches_the_oracle(cuda_device, oracle_lib, monk
     counts, visits, checksum, _ = saba_count(dg, 10, 64)
     want = oracle_lib.saba(idx, adj, 10, 64)
     assert np.array_equal(counts.astype(np.uint64), want)
+    dg.free()
+
+
+@pytest.mark.parametrize("hot,hot_rec", [("12288", "0"), ("12288", "1024"), ("8192", "4096"),
+                                         ("1024", "8192"), ("12288", "8192")])
+@pytest.mark.parametrize("wpl", ["1", "4"])
+def test_saba_shared_row_records_give_the_oracle_counters(cuda_device, oracle_lib, monkeypatch,
+                                                          hot, hot_rec, wpl):
+    """The plain walk copy with the highest-degree row records in shared memory: hops landing on
+    those numbers read the record there, the others from the copy in global memory (records are
+    capped at the shared counters' count, as in ("1024", "8192"))."""
+    from tgtp_b200 import synth
+    from tgtp_b200.aesc import AESCGraph, saba_count
+
+    monkeypatch.setenv("TGTP_SABA_INLINE", "0")
+    monkeypatch.setenv("TGTP_SABA_HOT", hot)
+    monkeypatch.setenv("TGTP_SABA_HOT_REC", hot_rec)
+    monkeypatch.setenv("TGTP_SABA_WPL", wpl)
+    g = synth.rmat(14, 8, 0.57, 0.19, 0.19, 3)
+    idx, adj = g.csr()
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, _, fb = saba_count(dg, 10, 64)
+    want = oracle_lib.saba(idx, adj, 10, 64)
+    assert np.array_equal(counts.astype(np.uint64), want)
+    assert visits == g.n * 64 * 10
     dg.free()

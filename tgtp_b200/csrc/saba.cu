@@ -154,13 +154,19 @@ __global__ void saba_scatter_kernel(const uint32_t* __restrict__ cnt, const uint
 // The walk on the renumbered graph.  Each lane carries WPL walkers (bouquets 4w + g of the warp's
 // step, g = lane / 8) whose hops are interleaved, so WPL independent load chains are in flight per
 // lane.  A warp takes a contiguous, equal share of the steps (4 WPL bouquets each).
+// The row records of the first `hot_rec` numbers (the highest degrees, which take most hops: on
+// R-MAT scale 18 the top 2,048 / 4,096 vertices hold 38 % / 52 % of the degree mass) are copied
+// into shared memory, so a hop that lands there makes one random L1/L2 load instead of two.
+// Shared memory: hot_rec 16-byte records, then `hot` 4-byte counters (hot_rec <= hot <= n).
 template <int WPL>
 __global__ void __launch_bounds__(kSabaThreads)
 saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict__ adjp,
                       uint32_t depth, uint32_t bouquets_per_src, uint32_t grid_step,
                       uint64_t total_bouquets, uint32_t* __restrict__ cnt, uint32_t hot,
-                      unsigned long long* __restrict__ fallback_total) {
-    extern __shared__ uint32_t s_cnt[];
+                      uint32_t hot_rec, unsigned long long* __restrict__ fallback_total) {
+    extern __shared__ uint4 s_rec[];
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_rec + hot_rec);
+    for (uint32_t i = threadIdx.x; i < hot_rec; i += blockDim.x) s_rec[i] = __ldg(info + i);
     for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
 
@@ -223,7 +229,9 @@ saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 if (active[w]) {
-                    const uint4 r = __ldg(info + nxt[w]);
+                    uint4 r;
+                    if (nxt[w] < hot_rec) r = s_rec[nxt[w]];
+                    else r = __ldg(info + nxt[w]);
                     beg[w] = r.x;
                     d[w] = r.y;
                     orig[w] = r.z;
@@ -446,6 +454,19 @@ bool saba_use_inline(const tgtp_graph* g) {
     return g->m * sizeof(uint4) <= size_t(48) << 20;
 }
 
+// Row records of the plain walk copy kept in shared memory (the highest-degree numbers): the tuned
+// choice (saba_tune, 1,024 << (code - 1) for code = bits 12-14 of the choice, 0 for none), else
+// TGTP_SABA_HOT_REC, else 2,048.
+uint32_t saba_hot_records(const tgtp_graph* g) {
+    if (g->saba_choice) {
+        const uint32_t code = (g->saba_choice >> 12) & 7u;
+        return code ? 1024u << (code - 1) : 0u;
+    }
+    if (const char* e = std::getenv("TGTP_SABA_HOT_REC"))
+        return uint32_t(std::max(0, std::min(std::atoi(e), 8192)));
+    return 2048u;
+}
+
 void saba_prepare_inline(tgtp_graph* g) {
     if (g->saba_inline_ready) return;
     saba_prepare(g);
@@ -468,8 +489,9 @@ void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step
     if (const char* e = std::getenv("TGTP_SABA_HOT")) cap = uint32_t(std::atoi(e));
     cap = std::max<uint32_t>(1024u, std::min<uint32_t>(cap, 53248u));
     const uint32_t hot = uint32_t(g->n < cap ? g->n : cap);
-    const size_t smem = sizeof(uint32_t) * hot;
     const bool inl = saba_use_inline(g);
+    const uint32_t hot_rec = inl ? 0u : std::min(hot, saba_hot_records(g));
+    const size_t smem = sizeof(uint32_t) * hot + sizeof(uint4) * hot_rec;
     if (inl) saba_prepare_inline(g);
     const void* kern = inl ? reinterpret_cast<const void*>(saba_walk_inline_kernel<WPL>)
                            : reinterpret_cast<const void*>(saba_walk_perm_kernel<WPL>);
@@ -489,7 +511,7 @@ void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step
     } else {
         saba_walk_perm_kernel<WPL><<<unsigned(blocks), kSabaThreads, smem, s>>>(
             g->saba_info.as<uint4>(), g->saba_adj.as<uint32_t>(), depth, bps, grid_step, total,
-            cnt, hot, fb);
+            cnt, hot, hot_rec, fb);
         TGTP_LAUNCH_CHECK("saba_walk_perm_kernel");
     }
 }
@@ -527,9 +549,10 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
 
 int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials) {
     std::vector<uint16_t> cand;
-    for (int inl : {1, 0}) {
-        if (inl && !saba_inline_fits(g)) continue;
-        for (int wpl : {1, 2, 4}) cand.push_back(uint16_t((inl ? 0x100 : 0) | wpl));
+    for (int wpl : {1, 2, 4}) {
+        if (saba_inline_fits(g)) cand.push_back(uint16_t(0x100 | wpl));
+        // plain copy: no hot records, or 2,048 / 4,096 of them in shared memory
+        for (int code : {0, 2, 3}) cand.push_back(uint16_t((code << 12) | wpl));
     }
     g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
     auto* c = g->counters.as<uint32_t>();
