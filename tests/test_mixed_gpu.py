@@ -155,3 +155,38 @@ def test_mixed_block_push_with_hbm_per_source_stage_gives_the_same_bits(manifest
         assert np.array_equal(got["0"][0].view(np.uint32), got["1"][0].view(np.uint32)), run
         assert got["0"][1] == got["1"][1], run
     g.free()
+
+
+def test_mixed_push_choice_is_learned_from_the_previous_run_without_a_counter_read(cuda_device,
+                                                                                   monkeypatch):
+    """Sparse Chung-Lu graph (28,000 ids, 120,000 edges, exponent 2.1): residual vectors beyond
+    shared memory, eps = 0.05.  The first run has no measurement and pushes per warp; its push
+    counters reach the handle through pinned memory, so the next run -- with no stats() call in
+    between -- takes the block push (frontiers averaging more than m / 40 traversals a round), with
+    the same bits."""
+    import torch
+
+    from tgtp_b200 import synth, workloads
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, PRECISION_MIXED, VEC_BF16
+
+    monkeypatch.delenv("TGTP_MIXED_BLOCK", raising=False)
+    monkeypatch.setenv("TGTP_KERNEL_DEADLINE_S", "120")
+    g = synth.chung_lu(28000, 120000, 2.1, 1)
+    idx, adj = g.csr()
+    values, v32, _ = workloads._eigenpairs(g, 128)
+    dg = AESCGraph.from_csr(idx, adj)
+    dg.upload_eigens(values, v32, VEC_BF16)
+    a = AESC(dg, AESCConfig(0.05, precision=PRECISION_MIXED, vec_dtype=VEC_BF16))
+    outs, kernels = [], []
+    for _ in range(3):
+        out = torch.empty(int(idx[-1]), dtype=torch.float32, device="cuda")
+        dg.set_profiling(True)
+        a.tgtp_device(out.data_ptr())
+        torch.cuda.synchronize()
+        kernels.append(set(dg.kernel_stats()))
+        dg.set_profiling(False)
+        outs.append(out.cpu().numpy())
+    assert "push_block" not in kernels[0] and "push_block" in kernels[1] and "push_block" in kernels[2]
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+    dg.free()

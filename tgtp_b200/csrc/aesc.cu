@@ -947,7 +947,6 @@ struct SourceParams {
     uint32_t* qbuf;       // 2 * n per warp
     WalkItem* items;      // max_degree per warp
     Real* pvec_g;         // n per warp (global tier)
-    unsigned long long* rbuf;  // n per warp: frontier residuals in fixed point (Jacobi push)
     unsigned long long* fx_g;  // n per warp: fixed-point accumulators (Jacobi push, global tier)
     unsigned char* wclean;     // per warp: 1 = its HBM vectors are all zero (left so by its last run)
     unsigned char* vis_g; // vis_stride per warp (global tier)
@@ -2262,31 +2261,15 @@ source_kernel(Pack pk) {
                 } else {
                     // ---- Jacobi push (mixed form) ----
                     // The frontier's residuals are taken together, in 2^-62 fixed point
-                    // (r_i = to_fixed(pvec[q_i]), pvec[q_i] = 0), then pushed over the concatenated
-                    // adjacency of 32 frontier vertices at a time: each lane walks entries lane,
-                    // lane + 32, ... with a cursor over the vertices' start offsets, and every entry
-                    // (v -> u) adds r_v to u's 64-bit accumulator with an integer atomic, so the sums
-                    // do not depend on the order.  The touched vertices form the new frontier in
-                    // discovery order; once the round is over their residuals become
+                    // (r_i = to_fixed(pvec[q_i]), pvec[q_i] = 0, read as each group of 32 frontier
+                    // vertices starts: the round's pushes go to the accumulators, never to pvec, so
+                    // every r_i is the value the round started with), then pushed over the
+                    // concatenated adjacency of 32 frontier vertices at a time: each lane walks
+                    // entries lane, lane + 32, ... with a cursor over the vertices' start offsets,
+                    // and every entry (v -> u) adds r_v to u's 64-bit accumulator with an integer
+                    // atomic, so the sums do not depend on the order.  The touched vertices form the
+                    // new frontier in discovery order; once the round is over their residuals become
                     // acc[u] / deg(u) (from_fixed), exactly as push_block_kernel computes them.
-                    unsigned long long* rfx = p0.rbuf + gw * size_t(sn);
-                    pipelined<uint32_t>(qs,
-                        [&](uint32_t i0, uint32_t* r) {
-#pragma unroll
-                            for (int b = 0; b < kB; ++b) {
-                                const uint32_t i = i0 + 32 * b + lane;
-                                r[b] = i < qs ? q[i] : NONE;
-                            }
-                        },
-                        [&](uint32_t i0, const uint32_t* r) {
-#pragma unroll
-                            for (int b = 0; b < kB; ++b) {
-                                if (r[b] == NONE) continue;
-                                rfx[i0 + 32 * b + lane] = to_fixed(float(pvec[r[b]]));
-                                pvec[r[b]] = Real(0);
-                            }
-                        });
-                    __syncwarp();
                     unsigned long long* rvs = acc + 64;
                     uint32_t* exs = reinterpret_cast<uint32_t*>(rvs + 32);
                     uint32_t* vbs = exs + 33;
@@ -2297,7 +2280,8 @@ source_kernel(Pack pk) {
                             const uint32_t v = q[i0 + lane];
                             vb = __ldg(idx + v);
                             vd = __ldg(idx + v + 1) - vb;
-                            rv = rfx[i0 + lane];
+                            rv = to_fixed(float(pvec[v]));
+                            pvec[v] = Real(0);
                         }
                         uint32_t incl = vd;
 #pragma unroll
@@ -2363,7 +2347,11 @@ source_kernel(Pack pk) {
                             });
                         __syncwarp();
                     }
-                    // the touched vertices' new residuals
+                    // the touched vertices' new residuals; in the same pass their flags are
+                    // cleared and their residual max / min taken (:484-491), which the GS push
+                    // does after the row update below (neither touches what it reads)
+                    mx = Real(0);
+                    mn = Real(1);
                     pipelined<uint32_t>(qns,
                         [&](uint32_t i0, uint32_t* r) {
 #pragma unroll
@@ -2376,8 +2364,12 @@ source_kernel(Pack pk) {
 #pragma unroll
                             for (int b = 0; b < kB; ++b) {
                                 if (r[b] == NONE) continue;
-                                pvec[r[b]] = Real(from_fixed(fx[r[b]], __ldg(p.deg + r[b])));
+                                const Real val = Real(from_fixed(fx[r[b]], __ldg(p.deg + r[b])));
+                                pvec[r[b]] = val;
                                 fx[r[b]] = 0ull;
+                                vis[r[b]] = 0;
+                                mx = std_max(mx, val);
+                                mn = std_min(mn, val);
                             }
                         });
                 }
@@ -2413,7 +2405,8 @@ source_kernel(Pack pk) {
                         });
                 }
                 // clear the new frontier's flags and take its residual max / min (:484-491; max and
-                // min do not depend on order)
+                // min do not depend on order); the Jacobi push did this with its new residuals
+                if constexpr (!JACOBI) {
                 mx = Real(0);
                 mn = Real(1);
                 pipelined<uint32_t>(qns,
@@ -2434,6 +2427,7 @@ source_kernel(Pack pk) {
                             mn = std_min(mn, val);
                         }
                     });
+                }
                 __syncwarp();
                 { uint32_t* tmp = q; q = qn; qn = tmp; }
                 qs = qns;
@@ -3107,6 +3101,14 @@ bool defer_to_batch(tgtp_graph* g, const tgtp_config& cfg, float* out, bool smem
 }
 
 // One tgtp() run.  Real = residual / eigen projection type, Acc = score accumulator,
+// Whether a warp's FP32 residual vector and flags (the mixed form's) exceed the 112 KB of the
+// shared-memory tier, so that the per-warp push works on vectors in HBM.
+bool mixed_beyond_smem(uint64_t n) {
+    return ((n * 4 + 15) & ~uint64_t(15)) + ((n + 15) & ~uint64_t(15)) + kAccBytes > uint64_t(112) * 1024;
+}
+void poll_push_hint(tgtp_graph* g);
+void post_push_hint(tgtp_graph* g, int key);
+
 // JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
 template <class Real, class Acc, bool JACOBI, class Vec>
 void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
@@ -3130,12 +3132,16 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     // block_ctas x kBlockCols listed sources (each wave has its own claim counter)
     // The block push gives the same bits as the per-warp push (fixed-point residual sums), so the
     // choice is only about speed: the handle's tuned layout, else TGTP_MIXED_BLOCK, else what the
-    // last completed mixed run on this graph measured (push_hint), else the per-warp push.
+    // last completed mixed run on this graph measured (push_hint), else the block push for
+    // vectors beyond shared memory at eps <= 0.01 (deep pushes: the block push was the faster one
+    // on every such graph measured) and the per-warp push otherwise.
     const int key = form_key(cfg);
+    if (JACOBI) poll_push_hint(g);
     bool block_mode = false;
     if (g->src_layout[key]) block_mode = JACOBI && (g->src_layout[key] & kLayoutBlock) != 0;
     else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
-    else block_mode = JACOBI && g->push_hint[key] == 2;
+    else if (g->push_hint[key]) block_mode = JACOBI && g->push_hint[key] == 2;
+    else block_mode = JACOBI && mixed_beyond_smem(n) && cfg.epsilon <= 0.01;
     g->last_key = key;
     // CTAs of the block push: one per SM, within a budget for their residual blocks of 24 GB or
     // half the device memory free now (beside what the blocks already hold), whichever is larger
@@ -3305,11 +3311,10 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t q_bytes = align(warps * 2 * size_t(n) * 4);
     const size_t it_bytes = align(warps * maxd * sizeof(WalkItem));
-    const size_t rb_bytes = JACOBI ? align(warps * size_t(n) * sizeof(unsigned long long)) : 0;
     const size_t pvg_bytes = use_smem ? 0 : align(warps * size_t(n) * sizeof(Real));
     const size_t visg_bytes = use_smem ? 0 : align(warps * vis_bytes);
     const size_t fxg_bytes = (JACOBI && !(use_smem && fx_in_smem)) ? align(warps * fx_bytes) : 0;
-    grow(g, g->scratch, q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
+    grow(g, g->scratch, q_bytes + it_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
     unsigned char* base = g->scratch.as<unsigned char>();
     SourceParams<Real, Acc> p;
     p.idx = g->idx.as<uint32_t>();
@@ -3324,8 +3329,6 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     base += q_bytes;
     p.items = reinterpret_cast<WalkItem*>(base);
     base += it_bytes;
-    p.rbuf = JACOBI ? reinterpret_cast<unsigned long long*>(base) : nullptr;
-    base += rb_bytes;
     p.pvec_g = use_smem ? nullptr : reinterpret_cast<Real*>(base);
     base += pvg_bytes;
     p.vis_g = use_smem ? nullptr : base;
@@ -3512,11 +3515,10 @@ void launch_group(BatchPlan& plan, BatchGroup& grp, cudaStream_t s, int num_sms)
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t q_bytes = align(warps * 2 * size_t(sn) * 4);
     const size_t it_bytes = align(warps * maxd * sizeof(WalkItem));
-    const size_t rb_bytes = JACOBI ? align(warps * size_t(sn) * sizeof(unsigned long long)) : 0;
     const size_t pvg_bytes = SMEM ? 0 : align(warps * size_t(sn) * sizeof(Real));
     const size_t visg_bytes = SMEM ? 0 : align(warps * vis_bytes);
     const size_t fxg_bytes = (JACOBI && !fx_in_smem) ? align(warps * fx_bytes) : 0;
-    grp.scratch.reserve(q_bytes + it_bytes + rb_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
+    grp.scratch.reserve(q_bytes + it_bytes + pvg_bytes + visg_bytes + fxg_bytes + 256);
     grp.wclean.reserve(warps + 16);
     const size_t packs = (grp.members.size() + kBatchPack - 1) / kBatchPack;
     grp.claims.reserve(sizeof(unsigned) * (packs + 1));
@@ -3535,8 +3537,6 @@ void launch_group(BatchPlan& plan, BatchGroup& grp, cudaStream_t s, int num_sms)
             b += q_bytes;
             p.items = reinterpret_cast<WalkItem*>(b);
             b += it_bytes;
-            p.rbuf = JACOBI ? reinterpret_cast<unsigned long long*>(b) : nullptr;
-            b += rb_bytes;
             p.pvec_g = SMEM ? nullptr : reinterpret_cast<Real*>(b);
             b += pvg_bytes;
             p.vis_g = SMEM ? nullptr : b;
@@ -3650,6 +3650,7 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
             } else {
                 fail(TGTP_ERR_INVALID_ARGUMENT, "MIXED form stores eigenvectors as F32 or BF16");
             }
+            post_push_hint(g, form_key(cfg));
             break;
         default:
             fail(TGTP_ERR_UNSUPPORTED, "unknown precision form");
@@ -3668,6 +3669,61 @@ void aesc_check_flags(tgtp_graph* g) {
         fail(TGTP_ERR_UNSUPPORTED, "a walk count exceeds the 32-bit walk grid");
 }
 
+namespace {
+
+// Mixed form: a dense round of the block push reads every slot once per 32 sources, about 40
+// times cheaper per slot than a per-warp push reads a frontier entry (scattered residual updates in
+// HBM).  So the block push pays off when a round's frontier averages more than m / 40 traversals
+// -- for graphs whose residual vectors do not fit in shared memory (smaller ones push per warp in
+// shared memory).  Measured on the sparse Chung-Lu graph (n = 25,860) at eps 0.05 / 0.01 / 0.005,
+// R-MAT (n = 143,522) at 0.05 / 0.01 and Chung-Lu (n = 199,772) at 0.05 / 0.01 / 0.005, the rule
+// picks the faster push every time (or one within 3 %).
+void learn_push_hint(tgtp_graph* g, int key, unsigned long long rounds,
+                     unsigned long long traversals) {
+    if (key < 2 || rounds == 0) return;
+    const double per_round = double(traversals) / double(rounds);
+    g->push_hint[key] = (mixed_beyond_smem(g->n) && per_round * 40.0 > double(g->m)) ? 2 : 1;
+}
+
+// The counters of a completed mixed run copied to pinned memory (see tgtp_graph::hint_host), if
+// that copy has finished; never waits.
+void poll_push_hint(tgtp_graph* g) {
+    if (g->hint_key < 0 || !g->hint_event) return;
+    const cudaError_t e = cudaEventQuery(g->hint_event);
+    if (e == cudaErrorNotReady) {
+        (void)cudaGetLastError();
+        return;
+    }
+    TGTP_CUDA(e);
+    unsigned long long rounds = 0, trav = 0;
+    for (int c = 0; c < kStStripes; ++c) {
+        rounds += g->hint_host[size_t(c) * kStCount + kStPushRounds];
+        trav += g->hint_host[size_t(c) * kStCount + kStPushTraversals];
+    }
+    learn_push_hint(g, g->hint_key, rounds, trav);
+    g->hint_key = -1;
+}
+
+// After a mixed run on the handle's stream (not while capturing): copy its counters to pinned
+// memory and record the event poll_push_hint looks at.
+void post_push_hint(tgtp_graph* g, int key) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TGTP_CUDA(cudaStreamIsCapturing(g->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return;
+    const size_t bytes = sizeof(unsigned long long) * kStCount * kStStripes;
+    if (!g->hint_host) {
+        void* h = nullptr;
+        TGTP_CUDA(cudaHostAlloc(&h, bytes, cudaHostAllocDefault));
+        g->hint_host = static_cast<unsigned long long*>(h);
+    }
+    if (!g->hint_event) TGTP_CUDA(cudaEventCreateWithFlags(&g->hint_event, cudaEventDisableTiming));
+    TGTP_CUDA(cudaMemcpyAsync(g->hint_host, g->stats.ptr, bytes, cudaMemcpyDeviceToHost, g->stream));
+    TGTP_CUDA(cudaEventRecord(g->hint_event, g->stream));
+    g->hint_key = key;
+}
+
+}  // namespace
+
 void aesc_read_stats(tgtp_graph* g, unsigned long long* st) {
     // the striped counters and the work words behind them, in one copy
     unsigned long long stripes[kStCount * kStStripes + 2];
@@ -3683,17 +3739,7 @@ void aesc_read_stats(tgtp_graph* g, unsigned long long* st) {
     for (int i = 0; i < kStCount; ++i) st[i] = 0;
     for (int c = 0; c < kStStripes; ++c)
         for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
-    // Mixed form: a dense round of the block push reads every slot once per 32 sources, about 40
-    // times cheaper per slot than a per-warp push reads a frontier entry (scattered residual
-    // updates in HBM).  So the block push pays off when a round's frontier averages more than
-    // m / 40 traversals -- for graphs whose residual vectors do not fit in shared memory (smaller
-    // ones push per warp in shared memory).
-    if (g->last_key >= 2 && st[kStPushRounds] > 0) {
-        const size_t per_warp = ((g->n * 4 + 15) & ~size_t(15)) + ((g->n + 15) & ~size_t(15)) + kAccBytes;
-        const double per_round = double(st[kStPushTraversals]) / double(st[kStPushRounds]);
-        g->push_hint[g->last_key] =
-            (per_warp > size_t(112) * 1024 && per_round * 40.0 > double(g->m)) ? 2 : 1;
-    }
+    learn_push_hint(g, g->last_key, st[kStPushRounds], st[kStPushTraversals]);
 }
 
 int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials) {

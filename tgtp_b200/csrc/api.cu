@@ -452,6 +452,8 @@ tgtp_graph::~tgtp_graph() {
     // the device buffers (members) are returned to the cache after this body, once the device
     // is idle; the stream goes back to the pool
     if (stream) cudaStreamSynchronize(stream);
+    if (hint_event) cudaEventDestroy(hint_event);
+    if (hint_host) cudaFreeHost(hint_host);
     if (own_stream) tgtp::stream_release(own_stream);
 }
 

@@ -177,6 +177,13 @@ struct tgtp_graph {
     // mixed form, per vector storage: 2 when the last completed run's frontiers were large enough
     // for the multi-source block push to pay off, 1 when not, 0 unknown
     uint8_t push_hint[4] = {0, 0, 0, 0};
+    // each mixed run also copies its two push counters into pinned host memory behind an event;
+    // the next run reads them there once the event has completed, so the hint is learned without
+    // the caller reading the counters and without a synchronisation (hint_key: form of the copy
+    // in flight, -1 none)
+    unsigned long long* hint_host = nullptr;
+    cudaEvent_t hint_event = nullptr;
+    int hint_key = -1;
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
