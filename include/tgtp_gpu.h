@@ -244,6 +244,16 @@ tgtp_status tgtp_graph_set_profiling(tgtp_graph* g, int enable);
 /* Copies up to `cap` entries; *count = entries available.  Synchronises the stream. */
 tgtp_status tgtp_graph_kernel_stats(tgtp_graph* g, tgtp_kernel_stat* out, int32_t cap,
                                     int32_t* count);
+/* Run trace, no counterpart in the reference (its per-source locals ell and nr,
+ * src/aesc.h:473-521, are not kept).  When on, every later run on the handle records the rounds
+ * pushed (ell) of each row that ran in the source kernel and the walk count nr of each walking
+ * slot; rows scored in closed form read 0 rounds, slots without walks 0.  Costs one store per row
+ * and per walking slot.  Not for runs captured into a batch. */
+tgtp_status tgtp_graph_set_trace(tgtp_graph* g, int enable);
+/* The trace of the handle's last run: host_walks m entries, host_rounds n entries (either may be
+ * NULL).  Synchronises the stream; TGTP_ERR_INVALID_ARGUMENT when the trace is off or no run has
+ * been made since it was turned on. */
+tgtp_status tgtp_graph_read_trace(tgtp_graph* g, uint32_t* host_walks, uint32_t* host_rounds);
 
 #ifdef __cplusplus
 }

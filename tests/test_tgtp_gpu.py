@@ -287,3 +287,36 @@ def test_config1_both_sequential_pushes_are_bit_exact(cuda_device, oracle_lib, c
     want64 = oracle_lib.tgtp(c["idx"], c["adj"], c["values"], c["v64"], 0.005, fp64=True)
     assert np.array_equal(got32.view(np.uint32), want32.view(np.uint32))
     assert np.array_equal(got64.view(np.uint32), want64.view(np.uint32))
+
+
+@pytest.mark.parametrize("form", ["fp32", "fp64", "mixed"])
+def test_run_trace_adds_up_to_the_run_counters(cuda_device, config1_inputs, form):
+    """The run trace (rounds pushed per row, walk count per slot) against the run's own counters
+    on the 4,039-vertex graph at eps = 0.005: the rounds of the rows that ran in the source kernel
+    plus one round per closed-form row are push_rounds, the walk counts sum to walk_count, the
+    walking slots are walk_edges; a row with walks pushed at least one round, and turning the
+    trace off leaves the scores as they were."""
+    from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_FP32, PRECISION_FP64,
+                                PRECISION_MIXED, VEC_F32, VEC_F64)
+
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    g.upload_eigens(c["values"], c["v64"], VEC_F64)
+    prec = {"fp32": PRECISION_FP32, "fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[form]
+    a = AESC(g, AESCConfig(0.005, precision=prec))
+    plain = a.tgtp()
+    g.set_trace(True)
+    traced = a.tgtp()
+    st = a.stats()
+    nr, ell = g.read_trace()
+    g.set_trace(False)
+    assert np.array_equal(plain.view(np.uint32), traced.view(np.uint32))
+    closed = int((ell == 0).sum())
+    assert int(ell.sum()) + closed == st["push_rounds"]
+    assert int(nr.astype(np.int64).sum()) == st["walk_count"]
+    assert int((nr > 0).sum()) == st["walk_edges"] > 0
+    rows = np.repeat(np.arange(c["n"]), np.diff(c["idx"].astype(np.int64)))
+    assert np.all(ell[rows[nr > 0]] >= 1)
+    assert np.all(nr[nr > 0] % 8 == 0)
+    g.free()

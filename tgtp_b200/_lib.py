@@ -91,6 +91,8 @@ SIGNATURES = {
     "tgtp_graph_set_profiling": (C.c_int, [_vp, C.c_int]),
     "tgtp_graph_kernel_stats": (C.c_int, [_vp, C.POINTER(KernelStat), C.c_int32,
                                           C.POINTER(C.c_int32)]),
+    "tgtp_graph_set_trace": (C.c_int, [_vp, C.c_int]),
+    "tgtp_graph_read_trace": (C.c_int, [_vp, _vp, _vp]),
 }
 
 _lib = None

@@ -138,6 +138,18 @@ class AESCGraph:
         return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms))
                 for i in range(min(cnt.value, 32))}
 
+    def set_trace(self, on: bool):
+        """Record, in every later run, the rounds pushed per row and the walk count per slot."""
+        check(lib().tgtp_graph_set_trace(self._h, 1 if on else 0))
+
+    def read_trace(self):
+        """(walk count per slot (m), rounds pushed per row (n)) of the last traced run; rows scored
+        in closed form and slots without walks read 0."""
+        nr = np.zeros(self.m, dtype=np.uint32)
+        ell = np.zeros(self.n, dtype=np.uint32)
+        check(lib().tgtp_graph_read_trace(self._h, nr.ctypes.data, ell.ctypes.data))
+        return nr, ell
+
     def free(self):
         if self._h is not None:
             check(lib().tgtp_graph_free(self._h))

@@ -975,6 +975,10 @@ struct SourceParams {
     // batch whose graphs share the scratch of one persistent launch).
     uint32_t scratch_n;
     bool gs_window;  // parity forms: the windowed sequential push (else one vertex at a time)
+    // Optional run trace (null when off): the walk count nr of every walking slot, and the rounds
+    // pushed (ell) of every listed row.
+    uint32_t* trace_nr;
+    uint32_t* trace_ell;
 };
 
 // The source kernel's parameters: one graph (N = 1), or up to N graphs whose listed rows one
@@ -2441,6 +2445,7 @@ source_kernel(Pack pk) {
             break;
         }
         if (!p.pre) st_rounds += ell;  // PrePush rounds are counted by push_block_kernel
+        if (p.trace_ell && lane == 0) p.trace_ell[src] = uint32_t(ell);
 
         // slots that still need walks (rest = tau - ell > 0), compacted in slot order
         uint32_t nitems = 0;
@@ -2715,6 +2720,7 @@ source_kernel(Pack pk) {
                         st_wh += nr * (unsigned long long)L;
                     }
                     items[my].nr = nr;
+                    if (p.trace_nr) p.trace_nr[items[my].pos] = uint32_t(nr);
                 }
                 __syncwarp();
             }
@@ -3356,6 +3362,14 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.stats = stats;
     p.adjd = g->adjd.as<uint2>();
     p.budget_ns = deadline_from_env();
+    p.trace_nr = p.trace_ell = nullptr;
+    if (g->trace_on) {
+        grow(g, g->trace, sizeof(uint32_t) * (m + n));
+        TGTP_CUDA(cudaMemsetAsync(g->trace.ptr, 0, sizeof(uint32_t) * (m + n), s));
+        p.trace_nr = g->trace.as<uint32_t>();
+        p.trace_ell = p.trace_nr + m;
+        g->trace_valid = true;
+    }
     p.pre = nullptr;
     p.pre_cols = nullptr;
     p.pre_final = nullptr;

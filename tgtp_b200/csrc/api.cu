@@ -671,6 +671,30 @@ tgtp_status tgtp_graph_set_profiling(tgtp_graph* g, int enable) {
     });
 }
 
+tgtp_status tgtp_graph_set_trace(tgtp_graph* g, int enable) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        g->trace_on = enable != 0;
+        g->trace_valid = false;
+    });
+}
+
+tgtp_status tgtp_graph_read_trace(tgtp_graph* g, uint32_t* host_walks, uint32_t* host_rounds) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        if (!g->trace_on || !g->trace_valid)
+            fail(TGTP_ERR_INVALID_ARGUMENT, "no traced run on this handle");
+        const auto* t = g->trace.as<uint32_t>();
+        if (host_walks)
+            TGTP_CUDA(cudaMemcpyAsync(host_walks, t, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost,
+                                      g->stream));
+        if (host_rounds)
+            TGTP_CUDA(cudaMemcpyAsync(host_rounds, t + g->m, sizeof(uint32_t) * g->n,
+                                      cudaMemcpyDeviceToHost, g->stream));
+        TGTP_CUDA(cudaStreamSynchronize(g->stream));
+    });
+}
+
 tgtp_status tgtp_graph_kernel_stats(tgtp_graph* g, tgtp_kernel_stat* out, int32_t cap,
                                     int32_t* count) {
     return guarded([&] {

@@ -181,6 +181,9 @@ struct tgtp_graph {
     // the next run reads them there once the event has completed, so the hint is learned without
     // the caller reading the counters and without a synchronisation (hint_key: form of the copy
     // in flight, -1 none)
+    // run trace (tgtp_graph_set_trace): m walk counts per slot, then n rounds per row
+    bool trace_on = false, trace_valid = false;
+    tgtp::DeviceBuffer trace;
     unsigned long long* hint_host = nullptr;
     cudaEvent_t hint_event = nullptr;
     int hint_key = -1;
