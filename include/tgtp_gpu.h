@@ -191,10 +191,10 @@ tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
 
 /* Times the walk layouts for this graph and walk configuration and keeps the fastest on the handle
  * for later saba_count calls: 1, 2 or 4 walkers per lane (4, 8 or 16 eight-lane bouquets per warp)
- * over the degree-renumbered walk copy, plain (with none, 2,048 or 4,096 of the highest-degree row
+ * over the degree-renumbered walk copy, plain (with none, 2,048 or 3,072 of the highest-degree row
  * records held in shared memory) or with the next row's record inlined in each slot.  `trials`
  * timed runs each after a warm-up.  *choice (may be NULL) receives the pick: low byte = walkers per
- * lane, 0x100 = inlined copy, bits 12-14 = c for 1,024 << (c - 1) shared row records (0: none).
+ * lane, 0x100 = inlined copy, bits 12-14 = c for 1,024 x c shared row records.
  * Counters are identical under every layout.  The reference has no counterpart (its OpenMP loop
  * has one layout). */
 tgtp_status saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t trials,

@@ -176,7 +176,7 @@ def test_saba_rmat18_static_entry_point_matches_the_fixture(cuda_device, rmat18,
 
 
 def test_saba_tuned_layout_gives_the_same_counters(cuda_device, oracle_lib):
-    """saba_tune times 1 / 2 / 4 walkers per lane over the plain walk copy (with 0 / 2,048 / 4,096
+    """saba_tune times 1 / 2 / 4 walkers per lane over the plain walk copy (with 0 / 2,048 / 3,072
     row records in shared memory) and the inlined one and keeps the fastest; every layout, and so
     the chosen one, gives the oracle's counters."""
     from tgtp_b200 import synth
@@ -213,8 +213,8 @@ def test_saba_every_walk_layout_matches_the_oracle(cuda_device, oracle_lib, monk
     dg.free()
 
 
-@pytest.mark.parametrize("hot,hot_rec", [("12288", "0"), ("12288", "1024"), ("8192", "4096"),
-                                         ("1024", "8192"), ("12288", "8192")])
+@pytest.mark.parametrize("hot,hot_rec", [("12288", "0"), ("12288", "1024"), ("12288", "3072"),
+                                         ("8192", "4096"), ("1024", "8192"), ("12288", "8192")])
 @pytest.mark.parametrize("wpl", ["1", "4"])
 def test_saba_shared_row_records_give_the_oracle_counters(cuda_device, oracle_lib, monkeypatch,
                                                           hot, hot_rec, wpl):

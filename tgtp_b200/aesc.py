@@ -244,7 +244,7 @@ def saba_count(g: AESCGraph, depth: int, n_walks: int, counters: bool = True):
 def saba_tune(g: AESCGraph, depth: int, n_walks: int, trials: int = 3) -> int:
     """Times the walk layouts for this graph and configuration and keeps the fastest on the
     handle; returns the choice (low byte: walkers per lane, 0x100: inlined walk copy, bits 12-14:
-    c for 1024 << (c - 1) row records in shared memory, 0 for none)."""
+    c for 1024 x c row records in shared memory)."""
     choice = C.c_int32(0)
     check(lib().saba_tune(g.handle, depth, n_walks, trials, C.byref(choice)))
     return int(choice.value)

@@ -2326,15 +2326,27 @@ source_kernel(Pack pk) {
                                 for (int b = 0; b < kB; ++b) {
                                     const bool valid = r[b].seg < 32u;
                                     const uint32_t u = r[b].u;
-                                    if (valid) atomicAdd(fx + u, rvs[r[b].seg]);
                                     // entries of one frontier vertex are distinct neighbours; only a
                                     // step that spans several vertices can repeat one, and then the
-                                    // first lane of a repeated neighbour discovers it
+                                    // first lane of a repeated neighbour adds the group's residuals
+                                    // (integers: any order gives the same sum) and discovers it.
+                                    // The accumulators are this warp's own, so with one writer per
+                                    // neighbour a step needs no atomics.
+                                    unsigned long long add = valid ? rvs[r[b].seg] : 0ull;
                                     const uint32_t seg0 = __shfl_sync(kFullMask, r[b].seg, 0);
                                     const bool one_seg = __all_sync(kFullMask, !valid || r[b].seg == seg0);
                                     const unsigned grp =
                                         one_seg ? (1u << lane) : __match_any_sync(kFullMask, u);
                                     const bool leader = valid && lane == uint32_t(__ffs(grp) - 1);
+                                    if (!one_seg) {
+                                        const unsigned others = __ballot_sync(kFullMask, valid && !leader);
+                                        for (unsigned mm = others; mm; mm &= mm - 1) {
+                                            const int t = __ffs(mm) - 1;
+                                            const unsigned long long ct = __shfl_sync(kFullMask, add, t);
+                                            if (leader && ((grp >> t) & 1u)) add += ct;
+                                        }
+                                    }
+                                    if (leader) fx[u] += add;
                                     bool fresh = false;
                                     if (leader && vis[u] == 0) {
                                         vis[u] = 1;
@@ -3718,9 +3730,11 @@ void poll_push_hint(tgtp_graph* g) {
     g->hint_key = -1;
 }
 
-// After a mixed run on the handle's stream (not while capturing): copy its counters to pinned
-// memory and record the event poll_push_hint looks at.
+// After a mixed run on the handle's stream (not while capturing) on a graph whose vectors exceed
+// shared memory (smaller ones always push per warp): copy its counters to pinned memory and
+// record the event poll_push_hint looks at.
 void post_push_hint(tgtp_graph* g, int key) {
+    if (!mixed_beyond_smem(g->n)) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     TGTP_CUDA(cudaStreamIsCapturing(g->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) return;

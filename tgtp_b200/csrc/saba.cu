@@ -455,16 +455,17 @@ bool saba_use_inline(const tgtp_graph* g) {
 }
 
 // Row records of the plain walk copy kept in shared memory (the highest-degree numbers): the tuned
-// choice (saba_tune, 1,024 << (code - 1) for code = bits 12-14 of the choice, 0 for none), else
-// TGTP_SABA_HOT_REC, else 2,048.
+// choice (saba_tune: 1,024 x bits 12-14 of the choice), else TGTP_SABA_HOT_REC, else 3,072.
+// Shared memory and L1 share 256 KB per SM: with the default 12,288 counters, 3,072 records make a
+// 96 KB block, two of which leave 60 KB of L1 for the walk copy; on R-MAT scale 18 (D 5 / 10 / 15,
+// W 2,048 / 16,384) that measured 1.09-1.11x the 2,048-record block and 1.06-1.28x no records
+// with one walker per lane, while any split that left under 32 KB of L1 (three 72 KB blocks, or
+// two of 104 KB) lost about a third.
 uint32_t saba_hot_records(const tgtp_graph* g) {
-    if (g->saba_choice) {
-        const uint32_t code = (g->saba_choice >> 12) & 7u;
-        return code ? 1024u << (code - 1) : 0u;
-    }
+    if (g->saba_choice) return 1024u * ((g->saba_choice >> 12) & 7u);
     if (const char* e = std::getenv("TGTP_SABA_HOT_REC"))
         return uint32_t(std::max(0, std::min(std::atoi(e), 8192)));
-    return 2048u;
+    return 3072u;
 }
 
 void saba_prepare_inline(tgtp_graph* g) {
@@ -530,7 +531,9 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
     g->saba_cnt.reserve(sizeof(uint32_t) * (g->n + 1));
     auto* cnt = g->saba_cnt.as<uint32_t>();
     TGTP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * g->n, s));
-    int wpl = 1;
+    // walkers per lane: the tuned choice, else TGTP_SABA_WPL, else 1 over the inlined copy and 2
+    // over the plain one (its two dependent loads per hop want more chains in flight)
+    int wpl = saba_use_inline(g) ? 1 : 2;
     if (g->saba_choice) wpl = g->saba_choice & 0xff;
     else if (const char* e = std::getenv("TGTP_SABA_WPL")) wpl = std::atoi(e);
     switch (wpl) {
@@ -551,7 +554,7 @@ int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials) {
     std::vector<uint16_t> cand;
     for (int wpl : {1, 2, 4}) {
         if (saba_inline_fits(g)) cand.push_back(uint16_t(0x100 | wpl));
-        // plain copy: no hot records, or 2,048 / 4,096 of them in shared memory
+        // plain copy: no hot records, or 2,048 / 3,072 of them in shared memory
         for (int code : {0, 2, 3}) cand.push_back(uint16_t((code << 12) | wpl));
     }
     g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
