@@ -69,8 +69,12 @@ def lib():
         L.oracle_walk2_f32.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint64,
                                        C.c_uint32, f32p]
         L.oracle_walk2_f32.restype = C.c_float
+        L.oracle_mt19937_nth.argtypes = [C.c_uint32, C.c_uint64]
+        L.oracle_mt19937_nth.restype = C.c_uint32
+        L.oracle_mt_walks.argtypes = [u32p, u32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, u64p,
+                                      C.c_int]
         for fn in (L.oracle_saba, L.oracle_taus_f32, L.oracle_taus_f64, L.oracle_tgtp_f32,
-                   L.oracle_tgtp_f64, L.oracle_parse_eigens):
+                   L.oracle_tgtp_f64, L.oracle_parse_eigens, L.oracle_mt_walks):
             fn.restype = C.c_int
         _lib = L
     return _lib
@@ -85,6 +89,22 @@ def saba(idx, adj, depth, n_walks, threads=0):
     n = len(idx) - 1
     out = np.zeros(n, dtype=np.uint64)
     rc = lib().oracle_saba(idx, adj, n, depth, n_walks, out, threads)
+    if rc:
+        raise ValueError("n_walks must be a multiple of 8")
+    return out
+
+
+def mt19937_nth(seed, k):
+    """The k-th draw (1-based) of std::mt19937 seeded with `seed`."""
+    return int(lib().oracle_mt19937_nth(seed, k))
+
+
+def mt_walks(idx, adj, depth, n_walks, simd=False, threads=0):
+    """Per-vertex visit counters (uint64) of the reference's MT19937 walk baseline (scalar or
+    8-lane bouquet draw order) from every vertex with a neighbour."""
+    n = len(idx) - 1
+    out = np.zeros(n, dtype=np.uint64)
+    rc = lib().oracle_mt_walks(idx, adj, n, depth, n_walks, 1 if simd else 0, out, threads)
     if rc:
         raise ValueError("n_walks must be a multiple of 8")
     return out

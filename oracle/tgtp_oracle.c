@@ -119,6 +119,99 @@ int oracle_saba(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint32_t d
     return 0;
 }
 
+/*
+ * std::mt19937, restated from Matsumoto & Nishimura, "Mersenne Twister: a 623-dimensionally
+ * equidistributed uniform pseudo-random number generator" (ACM TOMACS 8(1), 1998), with the C++
+ * standard's seeding (x_0 = seed, x_i = 1812433253 * (x_{i-1} ^ (x_{i-1} >> 30)) + i) and its
+ * tempering.  The reference's MT19937 walk runners draw from it (src/rw_experiment.cpp:39-47,
+ * src/rw_experiment_simd.cpp:54-59).
+ */
+typedef struct {
+    uint32_t x[624];
+    int next;
+} mt19937_state;
+
+static void mt19937_seed(mt19937_state* s, uint32_t seed) {
+    s->x[0] = seed;
+    for (uint32_t i = 1; i < 624; ++i) s->x[i] = 1812433253u * (s->x[i - 1] ^ (s->x[i - 1] >> 30)) + i;
+    s->next = 624;
+}
+
+static uint32_t mt19937_draw(mt19937_state* s) {
+    if (s->next >= 624) {
+        for (int i = 0; i < 624; ++i) {
+            const uint32_t y = (s->x[i] & 0x80000000u) | (s->x[(i + 1) % 624] & 0x7fffffffu);
+            s->x[i] = s->x[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        s->next = 0;
+    }
+    uint32_t y = s->x[s->next++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+uint32_t oracle_mt19937_nth(uint32_t seed, uint64_t k) {
+    mt19937_state s;
+    mt19937_seed(&s, seed);
+    uint32_t y = 0;
+    for (uint64_t i = 0; i < k; ++i) y = mt19937_draw(&s);
+    return y;
+}
+
+/*
+ * The reference's MT19937 walk baselines with integer counters: every source with a neighbour
+ * reseeds the generator with 42 + src (src/rw_experiment.cpp:110) and makes n_walks walks of
+ * exactly depth hops, each hop k = draw % degree(cur) (:39-47).  simd = 0: walk-major order (the
+ * scalar runner); simd = 1: bouquets of 8 walks stepping together, the 8 draws of a hop taken in
+ * lane order (src/rw_experiment_simd.cpp:44-83, n_walks a multiple of 8).  counters[v] = visits
+ * of v (start vertices not counted).
+ */
+int oracle_mt_walks(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint32_t depth,
+                    uint32_t n_walks, int simd, uint64_t* counters, int threads) {
+    if (simd && n_walks % 8 != 0) return -1;
+    memset(counters, 0, sizeof(uint64_t) * n);
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel
+    {
+        uint64_t* local = (uint64_t*)calloc(n, sizeof(uint64_t));
+        mt19937_state rng;
+#pragma omp for schedule(dynamic, 256)
+        for (long long src = 0; src < (long long)n; ++src) {
+            if (idx[src + 1] == idx[src]) continue;
+            mt19937_seed(&rng, 42u + (uint32_t)src);
+            if (!simd) {
+                for (uint32_t i = 0; i < n_walks; ++i) {
+                    uint32_t cur = (uint32_t)src;
+                    for (uint32_t len = 0; len < depth; ++len) {
+                        const uint32_t k = mt19937_draw(&rng) % (idx[cur + 1] - idx[cur]);
+                        cur = adj[idx[cur] + k];
+                        local[cur]++;
+                    }
+                }
+            } else {
+                for (uint32_t ii = 0; ii < n_walks; ii += 8) {
+                    uint32_t cur[8];
+                    for (int l = 0; l < 8; ++l) cur[l] = (uint32_t)src;
+                    for (uint32_t len = 0; len < depth; ++len) {
+                        uint32_t r[8];
+                        for (int l = 0; l < 8; ++l) r[l] = mt19937_draw(&rng);
+                        for (int l = 0; l < 8; ++l)
+                            cur[l] = adj[idx[cur[l]] + r[l] % (idx[cur[l] + 1] - idx[cur[l]])];
+                        for (int l = 0; l < 8; ++l) local[cur[l]]++;
+                    }
+                }
+            }
+        }
+#pragma omp critical
+        for (uint64_t v = 0; v < n; ++v) counters[v] += local[v];
+        free(local);
+    }
+    return 0;
+}
+
 /* k-th largest value (1-based, counting multiplicity) by quickselect; destroys a[]. */
 #define DEFINE_KTH(T, NAME)                                                              \
     static T NAME(T* a, uint64_t size, uint64_t k) {                                     \

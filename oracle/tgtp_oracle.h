@@ -5,6 +5,7 @@
  *
  * A plain-C restatement of the reference's hot path:
  *   - SABA one-way walk counter        src/rw_experiment_saba.cpp:65-145 (integer counters)
+ *   - MT19937 walk baselines           src/rw_experiment.cpp:34-47, rw_experiment_simd.cpp:44-83
  *   - calculate_taus / get_tau /
  *     get_delta / get_upsilon          src/aesc.h:129-216
  *   - tgtp_baseline (push, stop test,
@@ -38,6 +39,15 @@ typedef struct {
 /* SABA counters: counters[v] = visits of v over all sources (start vertex not counted). */
 int oracle_saba(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint32_t depth,
                 uint32_t n_walks, uint64_t* counters, int threads);
+
+/* The k-th draw (1-based) of std::mt19937 seeded with `seed` (known answer: seed 5489, k 10000
+ * gives 4123659995, the C++ standard's check value). */
+uint32_t oracle_mt19937_nth(uint32_t seed, uint64_t k);
+
+/* MT19937 walk baselines src/rw_experiment.cpp:34-47 (simd = 0) and
+ * src/rw_experiment_simd.cpp:44-83 (simd = 1), integer counters; -1 if simd and n_walks % 8. */
+int oracle_mt_walks(const uint32_t* idx, const uint32_t* adj, uint64_t n, uint32_t depth,
+                    uint32_t n_walks, int simd, uint64_t* counters, int threads);
 
 /* Per-CSR-slot walk-length bound tau (src/aesc.h:164-216), epsilon = eps/2 as the caller passes. */
 int oracle_taus_f32(const uint32_t* idx, const uint32_t* adj, uint64_t n, const double* values,

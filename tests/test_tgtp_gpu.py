@@ -199,6 +199,12 @@ def test_invalid_arguments_are_rejected(manifest, cuda_device):
         g.upload_eigens(np.array([1.0, 0.5]), np.zeros(8, np.float32))
         AESC(g, AESCConfig(0.05, omega=2)).tgtp()
     g.free()
+    # an edge into a vertex without neighbours (a walk would have nowhere to go): refused at upload
+    for idx, adj in ((np.array([0, 1, 1], np.uint32), np.array([1], np.uint32)),
+                     (np.array([0, 2, 3, 3], np.uint32), np.array([1, 2, 0], np.uint32))):
+        with pytest.raises(TgtpError) as e:
+            AESCGraph.from_csr(idx, adj)
+        assert e.value.status == 1 and "without neighbours" in str(e.value)
 
 
 def test_fp64_bulk_copy_tau_gives_the_same_bits(manifest, cuda_device, oracle_lib, monkeypatch):

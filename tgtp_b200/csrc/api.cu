@@ -217,6 +217,7 @@ __global__ void validate_kernel(const uint32_t* __restrict__ idx, const uint32_t
          q += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t a = adj[q];
         if (a >= n) flags |= 1u;
+        else if (idx[a + 1] == idx[a]) flags |= 8u;  // a walk would stop at a vertex without neighbours
         if (q > idx[row_of[q]]) {
             const uint32_t b = adj[q - 1];
             if (a < b) flags |= 2u;
@@ -418,6 +419,7 @@ void graph_prepare(tgtp_graph* g) {
     TGTP_CUDA(cudaStreamSynchronize(s));
     if (h[1] & 1u) fail(TGTP_ERR_INVALID_ARGUMENT, "neighbour id out of range");
     if (h[1] & 2u) fail(TGTP_ERR_INVALID_ARGUMENT, "rows must be sorted");
+    if (h[1] & 8u) fail(TGTP_ERR_INVALID_ARGUMENT, "an edge leads to a vertex without neighbours");
     g->has_multi_edges = (h[1] & 4u) != 0;
     g->max_degree = h[2];
     g->min_degree = h[3];
