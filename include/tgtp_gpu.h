@@ -15,6 +15,8 @@
  *   AESCConfig{epsilon,delta,omega,gamma} src/aesc.h:98-102    -> tgtp_config
  *   float* AESC::tgtp()                 src/aesc.h:120-127     -> tgtp_run / tgtp_run_device
  *   saba_randomwalk + runner reduction  src/rw_experiment_saba.cpp:65-145,186-208 -> saba_count
+ *   scalar_randomwalk + runner reduction src/rw_experiment.cpp:34-47,88-118      -> mt_walk_count(0)
+ *   simd_randomwalk + runner reduction  src/rw_experiment_simd.cpp:44-83,128-156  -> mt_walk_count(1)
  *   AESCGraph::free / graph_t::free     src/aesc.h:93-96, src/graph.h:22-28 -> tgtp_graph_free
  *   exception -> "tgtp: msg", exit 1    src/main.cpp:46-49     -> tgtp_status + tgtp_last_error
  */
@@ -199,6 +201,17 @@ tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
  * has one layout). */
 tgtp_status saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t trials,
                       int32_t* choice);
+
+/* ---- MT19937 walk baselines ------------------------------------------------------------------ */
+/* The reference's comparison walks: from every vertex with a neighbour, n_walks walks of `depth`
+ * hops with std::mt19937 reseeded to 42 + src and k = draw % degree per hop; simd = 0 takes the
+ * scalar runner's draw order (walk-major, src/rw_experiment.cpp:34-47), simd = 1 the AVX2 runner's
+ * (bouquets of 8 walks, the 8 draws of a hop in lane order, src/rw_experiment_simd.cpp:44-83;
+ * n_walks a multiple of 8).  counters[v] = visits of v (start vertex excluded), exact uint32
+ * (the reference's float counters stop at 2^24 per thread); host_counters (n uint32) may be NULL;
+ * out->fallback_bouquets is 0.  Synchronous. */
+tgtp_status mt_walk_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t simd,
+                          uint32_t* host_counters, saba_result* out);
 
 /* No counterpart in the reference: the walk counter for callers that cannot allocate device
  * memory, e.g. a process whose device memory is owned by another allocator or budget, or a

@@ -285,3 +285,44 @@ def test_saba_rmat18_fixture_is_reproduced_by_the_oracle(oracle_lib):
     got = oracle_lib.saba(idx, adj, 5, 2048)
     assert sha256_u32(got) == cell["counters_sha256"]
     assert int((got * np.arange(1, g.n + 1, dtype=np.uint64)).sum()) == cell["checksum"]
+
+
+def test_mt19937_restatement_known_answers(oracle_lib):
+    """std::mt19937 restated in the oracle: the C++ standard's check value (the 10,000th draw of the
+    default seed 5489 is 4123659995) and the first draws of the walk runners' seed 42."""
+    assert oracle_lib.mt19937_nth(5489, 10000) == 4123659995
+    assert oracle_lib.mt19937_nth(5489, 1) == 3499211612
+    assert [oracle_lib.mt19937_nth(42, k) for k in (1, 2, 3)] == [1608637542, 3421126067, 4083286876]
+
+
+@pytest.mark.parametrize("simd", [False, True])
+@pytest.mark.parametrize("graph,depth,walks", [("config1", 5, 64), ("rmat14", 10, 24),
+                                               ("rmat12", 100, 8), ("rmat12", 700, 8)])
+def test_mt_walk_oracle_matches_the_reference_walks(tmp_path, oracle_lib, tgtp_lib, simd, graph,
+                                                    depth, walks):
+    """The MT19937 walk baselines: every counter of the oracle equal to the reference's own walk
+    routine (scalar_randomwalk / simd_randomwalk, run by oracle/_ref/mt_harness_O2 and
+    mt_simd_harness_O2 with std::mt19937 reseeded to 42 + src as the runners do)."""
+    import subprocess
+
+    from conftest import ROOT
+    from tgtp_b200 import synth
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "mt_simd_harness_O2" if simd else "mt_harness_O2")
+    if not os.path.exists(exe):
+        pytest.skip("the reference binaries are not built (oracle/_ref)")
+    g = {"config1": lambda: synth.config1_graph(1),
+         "rmat14": lambda: synth.rmat(14, 8, 0.57, 0.19, 0.19, 3),
+         "rmat12": lambda: synth.rmat(12, 8, 0.57, 0.19, 0.19, 5)}[graph]()
+    synth.write_graph_txt(g, str(tmp_path / "graph.txt"))
+    out = tmp_path / "counts.u32"
+    r = subprocess.run([exe, str(tmp_path / "graph.txt"), str(depth), str(walks), str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    want = np.fromfile(out, dtype=np.uint32).astype(np.uint64)
+    idx, adj = g.csr()
+    got = oracle_lib.mt_walks(idx, adj, depth, walks, simd=simd)
+    assert np.array_equal(got, want)
+    n, m, visits, checksum = (int(x) for x in r.stdout.split())
+    assert (n, m) == (g.n, len(adj)) and visits == int(got.sum())
+    assert checksum == int((got * np.arange(1, n + 1, dtype=np.uint64)).sum())

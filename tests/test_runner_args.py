@@ -1,6 +1,7 @@
 """The drop-in executables' argument handling on the CPU: every rejected command line exits 1 with
 the reference runner's message (src/main.cpp:9-31, src/benchmark.cpp:10-28 with
-src/benchmark_options.h, src/rw_experiment_saba.cpp:150-163), checked before any device work.
+src/benchmark_options.h, src/rw_experiment_saba.cpp:150-163, src/rw_experiment.cpp:52-57,
+src/rw_experiment_simd.cpp:88-100), checked before any device work.
 The expected messages are pinned here; where the reference binaries built under oracle/_ref are
 present (the -O2 parity builds for tgtp and benchmark: the -Ofast build drops tgtp's isfinite
 test), each case is also run through them and must give the same exit code and output."""
@@ -66,6 +67,12 @@ SABA_CASES = [
 ]
 
 
+MT_SIMD_CASES = [
+    (["f", "d", "5", "12"], "n_walks must be a multiple of 8"),
+    (["f", "d", "5", "4", "4"], "n_walks must be a multiple of 8"),
+]
+
+
 @pytest.fixture(scope="module")
 def runners(tgtp_lib):
     from tgtp_b200 import build
@@ -102,8 +109,15 @@ def test_rw_experiment_saba_rejects_like_the_reference(runners, tmp_path, args, 
     _check(runners, tmp_path, "rw_experiment_saba", "rw_experiment_saba", args, message)
 
 
+@pytest.mark.parametrize("args,message", MT_SIMD_CASES)
+def test_rw_experiment_simd_rejects_like_the_reference(runners, tmp_path, args, message):
+    _check(runners, tmp_path, "rw_experiment_simd", "rw_experiment_simd", args, message)
+
+
 @pytest.mark.parametrize("name,args", [("tgtp", []), ("tgtp", ["a"] * 7), ("benchmark", []),
-                                       ("rw_experiment_saba", ["f", "d", "5"])])
+                                       ("rw_experiment_saba", ["f", "d", "5"]),
+                                       ("rw_experiment", ["f", "d", "5"]),
+                                       ("rw_experiment_simd", [])])
 def test_usage_lines(runners, tmp_path, name, args):
     exe = os.path.join(runners, name)
     rc, out, err = _run(exe, args, tmp_path)
@@ -120,11 +134,18 @@ def test_usage_lines(runners, tmp_path, name, args):
         assert (rrc, rout, rerr.replace(ref, exe)) == (rc, out, err)
 
 
-def test_rw_experiment_saba_reports_an_unreadable_graph(runners, tmp_path):
+@pytest.mark.parametrize("name", ["rw_experiment_saba", "rw_experiment", "rw_experiment_simd"])
+def test_walk_runners_report_an_unreadable_graph(runners, tmp_path, name):
     # the reference lets this exception escape (the process aborts); here it is a message and exit 1
-    rc, out, err = _run(os.path.join(runners, "rw_experiment_saba"), ["nofolder", "ds", "5", "16"],
-                        tmp_path)
-    assert (rc, out, err) == (1, "", "rw_experiment_saba: cannot open graph: nofolder/ds/graph.txt")
+    rc, out, err = _run(os.path.join(runners, name), ["nofolder", "ds", "5", "16"], tmp_path)
+    assert (rc, out, err) == (1, "", f"{name}: cannot open graph: nofolder/ds/graph.txt")
+
+
+@pytest.mark.parametrize("name", ["rw_experiment", "rw_experiment_simd"])
+def test_mt_walk_runners_refuse_counts_beyond_32_bits(runners, tmp_path, name):
+    """The reference would start 2^33 walks per vertex; the GPU runners take 32-bit counts."""
+    rc, out, err = _run(os.path.join(runners, name), ["f", "d", "5", "8589934592"], tmp_path)
+    assert (rc, out, err) == (1, "", "depth and n_walks must fit in 32 bits")
 
 
 @pytest.mark.parametrize("name,args", [("tgtp", ["x", "y", "0.05", "16", "10", "o"]),

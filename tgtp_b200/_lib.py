@@ -92,6 +92,7 @@ SIGNATURES = {
     "tgtp_graph_kernel_stats": (C.c_int, [_vp, C.POINTER(KernelStat), C.c_int32,
                                           C.POINTER(C.c_int32)]),
     "tgtp_graph_set_trace": (C.c_int, [_vp, C.c_int]),
+    "mt_walk_count": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_int32, _vp, C.POINTER(SabaResult)]),
     "tgtp_graph_read_trace": (C.c_int, [_vp, _vp, _vp]),
 }
 

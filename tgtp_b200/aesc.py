@@ -241,6 +241,17 @@ def saba_count(g: AESCGraph, depth: int, n_walks: int, counters: bool = True):
     return out, int(res.visit_count), int(res.checksum), int(res.fallback_bouquets)
 
 
+def mt_walk_count(g: AESCGraph, depth: int, n_walks: int, simd: bool = False,
+                  counters: bool = True):
+    """The reference's MT19937 walk baselines (scalar or, with simd, 8-lane bouquet draw order):
+    (counters uint32[n] | None, visit_count, checksum)."""
+    out = np.empty(g.n, np.uint32) if counters else None
+    res = _lib.SabaResult()
+    check(lib().mt_walk_count(g.handle, depth, n_walks, 1 if simd else 0,
+                              ptr(out) if out is not None else None, C.byref(res)))
+    return out, int(res.visit_count), int(res.checksum)
+
+
 def saba_tune(g: AESCGraph, depth: int, n_walks: int, trials: int = 3) -> int:
     """Times the walk layouts for this graph and configuration and keeps the fastest on the
     handle; returns the choice (low byte: walkers per lane, 0x100: inlined walk copy, bits 12-14:

@@ -32,10 +32,13 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-I" + INCLUDE, "-I" + CSRC,
              "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["api.cu", "saba.cu", "aesc.cu", "batch.cu", "exact_sc.cu"]
+CU_SOURCES = ["api.cu", "saba.cu", "aesc.cu", "batch.cu", "exact_sc.cu", "mt_walk.cu"]
 CPP_SOURCES = ["host_io.cpp"]
-RUNNERS = {"tgtp": "tgtp_main.cpp", "benchmark": "benchmark_main.cpp",
-           "rw_experiment_saba": "rw_experiment_saba_main.cpp"}
+# executable -> (source under csrc/host, extra flags)
+RUNNERS = {"tgtp": ("tgtp_main.cpp", []), "benchmark": ("benchmark_main.cpp", []),
+           "rw_experiment_saba": ("rw_experiment_saba_main.cpp", []),
+           "rw_experiment": ("rw_experiment_main.cpp", []),
+           "rw_experiment_simd": ("rw_experiment_main.cpp", ["-DTGTP_MT_SIMD"])}
 
 
 def _headers():
@@ -86,14 +89,14 @@ def build(force: bool = False, verbose: bool = False, runners: bool = True) -> s
                                                              "-lpthread", "-ldl"], verbose)
     if runners:
         os.makedirs(BIN, exist_ok=True)
-        for name, src in RUNNERS.items():
+        for name, (src, flags) in RUNNERS.items():
             s = os.path.join(CSRC, "host", src)
             if not os.path.exists(s):
                 continue
             exe = os.path.join(BIN, name)
             if force or _stale(exe, [s, LIB] + headers):
-                _run(["g++"] + CXX_FLAGS + ["-o", exe, s, "-L" + PKG, "-ltgtp_gpu",
-                                            "-Wl,-rpath,$ORIGIN/.."], verbose)
+                _run(["g++"] + CXX_FLAGS + flags + ["-o", exe, s, "-L" + PKG, "-ltgtp_gpu",
+                                                    "-Wl,-rpath,$ORIGIN/.."], verbose)
     return LIB
 
 

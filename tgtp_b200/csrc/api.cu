@@ -661,6 +661,29 @@ tgtp_status saba_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t
     });
 }
 
+tgtp_status mt_walk_count(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int32_t simd,
+                          uint32_t* host_counters, saba_result* out) {
+    return guarded([&] {
+        if (!g) fail(TGTP_ERR_INVALID_ARGUMENT, "null graph");
+        if (simd && n_walks % 8 != 0) fail(TGTP_ERR_INVALID_ARGUMENT, "n_walks must be a multiple of 8");
+        g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
+        auto* c = g->counters.as<uint32_t>();
+        mt_walk_run(g, depth, n_walks, simd != 0, c);
+        uint64_t sums[3];
+        saba_summarize(g, c, sums);
+        if (host_counters)
+            TGTP_CUDA(cudaMemcpy(host_counters, c, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost));
+        if (out) {
+            out->visit_count = sums[0];
+            out->checksum = sums[1];
+            out->fallback_bouquets = 0;
+        }
+        const unsigned __int128 expect = (unsigned __int128)g->num_active * n_walks * depth;
+        if ((unsigned __int128)sums[0] != expect)
+            fail(TGTP_ERR_OVERFLOW, "a uint32 visit counter overflowed");
+    });
+}
+
 tgtp_status tgtp_release_cached_memory(void) {
     return guarded([&] { cache_trim(); });
 }

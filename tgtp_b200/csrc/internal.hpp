@@ -219,6 +219,9 @@ void saba_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, uint32_t* device_
 // walk configuration, `trials` runs each after a warm-up, and keeps the fastest on the handle.
 int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials);
 void saba_summarize(tgtp_graph* g, const uint32_t* device_counters, uint64_t* host_sums3);
+// The reference's MT19937 walk baselines (scalar or 8-lane bouquet draw order) into
+// device_counters (n uint32), asynchronous; the sums of saba_summarize then describe them.
+void mt_walk_run(tgtp_graph* g, uint32_t depth, uint32_t n_walks, bool simd, uint32_t* device_counters);
 void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores);
 // Times the candidate source-kernel layouts of cfg's form on this graph (trials runs each, after
 // one warm-up) and keeps the fastest on the handle.  Returns the chosen layout code.
