@@ -15,7 +15,7 @@ from conftest import GOLDEN, ROOT
 def _declared_functions():
     text = open(os.path.join(ROOT, "include", "tgtp_gpu.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(tgtp_\w+|saba_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(tgtp_\w+|saba_\w+|mt_walk_\w+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol(tgtp_lib):
