@@ -184,14 +184,16 @@ def cpu_reference_run(folder_root: str, dataset: str, threads: int, repeats: int
     return secs
 
 
-def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3):
-    """The reference's rw_experiment_saba (built from its sources into oracle/_ref) on `g`, on all
-    host cores: the fastest of `runs` runs, as transitions per second of its own walk timer, or None
-    when the binary is missing or fails."""
+def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3,
+                       binary: str = "rw_experiment_saba"):
+    """The reference's walk runner `binary` (rw_experiment_saba, or the MT19937 rw_experiment /
+    rw_experiment_simd; built from its sources into oracle/_ref) on `g`, on all host cores: the mean
+    of `runs` runs, as transitions per second of its own walk timer, or None when the binary is
+    missing or fails."""
     import oracle
     from tgtp_b200 import synth
 
-    exe = oracle.ref_binary("rw_experiment_saba")
+    exe = oracle.ref_binary(binary)
     if exe is None:
         return None
     folder = os.path.join(root, "saba_data")
@@ -213,7 +215,7 @@ def saba_cpu_reference(g, root: str, depth: int, walks: int, runs: int = 3):
     total = walk_s[0][1]
     return {"transitions_per_s": total / t_rw, "transitions": total, "cores": threads,
             "omp_num_threads": threads, "walk_seconds": t_rw,
-            "sample": f"mean of {runs} runs of the reference rw_experiment_saba (-Ofast, OpenMP) "
+            "sample": f"mean of {runs} runs of the reference {binary} (-Ofast, OpenMP) "
                       "on the same graph"}
 
 
@@ -258,6 +260,29 @@ def saba_rmat18(hbm: float, peak_kind: str, root: str, with_cpu: bool):
                           "hbm_frac_of_" + peak_kind: tr_c * 20 / (ms_c * 1e-3) / 1e9 / hbm,
                           "visit_count": vc_c, "checksum": cs_c})
     out["cells"] = cells
+    # the MT19937 comparison walks (src/rw_experiment.cpp, src/rw_experiment_simd.cpp), D 5, W 2,048
+    from tgtp_b200.aesc import mt_walk_count
+
+    mt = {}
+    for simd in (False, True):
+        mt_walk_count(dg, 5, 2048, simd=simd, counters=False)
+        dg.set_profiling(True)
+        for _ in range(3):
+            _, vc_m, cs_m = mt_walk_count(dg, 5, 2048, simd=simd, counters=False)
+        ks_m = dg.kernel_stats()
+        dg.set_profiling(False)
+        ms_m = ks_m["mt_walk"][1] / ks_m["mt_walk"][0]
+        tr_m = g.n * 2048 * 5
+        cell_m = {"kernel_ms": ms_m, "transitions_per_s": tr_m / (ms_m * 1e-3),
+                  "hbm_frac_of_" + peak_kind: tr_m * 20 / (ms_m * 1e-3) / 1e9 / hbm,
+                  "visit_count": vc_m, "checksum": cs_m}
+        if with_cpu:
+            ref_m = saba_cpu_reference(g, root, 5, 2048, runs=1,
+                                       binary="rw_experiment_simd" if simd else "rw_experiment")
+            if ref_m is not None:
+                cell_m["cpu_reference"] = ref_m
+        mt["simd" if simd else "regular"] = cell_m
+    out["mt19937_walks"] = mt
     dg.free()
     if with_cpu:
         ref = saba_cpu_reference(g, root, 5, 2048)
