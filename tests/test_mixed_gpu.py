@@ -190,3 +190,43 @@ def test_mixed_push_choice_is_learned_from_the_previous_run_without_a_counter_re
     for o in outs[1:]:
         assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
     dg.free()
+
+
+def test_mixed_and_fp64_differ_only_on_slots_next_to_a_pushed_row(cuda_device):
+    """Where the two forms' scores part, per slot (batch graphs of the batched workload, own eps):
+    a slot both of whose rows finish in closed form in both forms (no round past the first, no
+    walk; the run trace reads 0 rounds) agrees to float rounding (1e-6 relative); every larger
+    difference sits on a slot one of whose rows pushed.  The mixed form's Jacobi rounds and the
+    FP64 form's Gauss-Seidel rounds leave different residuals, so such slots differ even when
+    their tau, rounds and walk counts agree; both stay within eps of the exact value at the same
+    rate (tests/test_exact_sc_gpu.py)."""
+    from tgtp_b200 import eigenprep_gpu, synth
+    from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_FP64, PRECISION_MIXED,
+                                VEC_BF16, VEC_F64)
+
+    work = sorted(synth.config5_graphs(5, 64), key=lambda ge: ge[0].n)[:6]
+    pushed_total = 0
+    for g, eps in work:
+        idx, adj = g.csr()
+        vals, vecs, _, _, _ = eigenprep_gpu.compute(g.n, g.u, g.v, 128, seed=1, tol=1e-6,
+                                                    max_iter=60)
+        v64 = np.ascontiguousarray(vecs.T).ravel()
+        dg = AESCGraph.from_csr(idx, adj)
+        dg.upload_eigens(vals, v64, VEC_F64)
+        dg.upload_eigens(vals, v64.astype(np.float32), VEC_BF16)
+        dg.set_trace(True)
+        out = {}
+        for label, cfg in (("fp64", AESCConfig(eps, precision=PRECISION_FP64)),
+                           ("mixed", AESCConfig(eps, precision=PRECISION_MIXED,
+                                                vec_dtype=VEC_BF16))):
+            s = AESC(dg, cfg).tgtp().astype(np.float64)
+            out[label] = (s, dg.read_trace()[1])
+        dg.free()
+        rows = np.repeat(np.arange(g.n), np.diff(idx.astype(np.int64)))
+        closed = (out["fp64"][1] == 0) & (out["mixed"][1] == 0)
+        both_closed = closed[rows] & closed[adj]
+        dev = np.abs(out["mixed"][0] - out["fp64"][0]) / np.abs(out["fp64"][0])
+        assert np.all(dev[both_closed] <= 1e-6), (g.n, float(dev[both_closed].max()))
+        assert np.all(~both_closed[dev > 1e-6])
+        pushed_total += int((~both_closed).sum())
+    assert pushed_total > 0

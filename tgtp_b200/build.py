@@ -6,7 +6,7 @@
 
 Outputs (git-ignored, they travel with the tree):
     tgtp_b200/libtgtp_gpu.so
-    tgtp_b200/bin/{tgtp,benchmark,rw_experiment_saba}
+    tgtp_b200/bin/{tgtp,benchmark,rw_experiment_saba,rw_experiment,rw_experiment_simd}
 """
 from __future__ import annotations
 

@@ -923,7 +923,7 @@ tau_bound_kernel(const uint4* __restrict__ fedge, uint64_t num_forward,
 
 // ---- stage 2: per-source push, edge bound and walks -----------------------------------------------
 struct WalkItem {
-    uint32_t pos, v, len, pad;
+    uint32_t pos, v, len, pad;  // pad: in a walk queue, the item's list entry (its source)
     unsigned long long nr;
 };
 
@@ -979,6 +979,10 @@ struct SourceParams {
     // pushed (ell) of every listed row.
     uint32_t* trace_nr;
     uint32_t* trace_ell;
+    // PrePush mode: when set, a source's walking slots (with their nr) are appended to this queue
+    // (walk_count counts them) and walk_queue_kernel walks them, instead of the warp here
+    WalkItem* walk_queue;
+    unsigned* walk_count;
 };
 
 // The source kernel's parameters: one graph (N = 1), or up to N graphs whose listed rows one
@@ -1250,6 +1254,11 @@ __device__ __forceinline__ void seg_maxmin(uint32_t seg, Real& mx, Real& mn) {
 // column holds its source's final residual vector; the edge bound, chi and walks of those sources
 // then run in source_kernel (PrePush mode), which copies the column into its own residual vector.
 constexpr int kBlockCols = 32;
+// rows a warp of push_block_kernel claims at a time (their dependent loads are issued together).
+// Measured on three graphs (n = 25,860 / 143,522 / 199,772): 1 row is 3-6 % faster than the plain
+// loop (the row's own value and first adjacency chunk are requested before its neighbours are
+// read), 2 and 4 rows 0-25 % slower (the kernel is at its 64-register cap).
+constexpr int kRowBatch = 1;
 
 
 struct PushBlockParams {
@@ -1532,7 +1541,7 @@ push_block_kernel(PushBlockParams p) {
         if (threadIdx.x == 0) {
             s_ln = 0;
             s_live_deg = 0;
-            s_next = nwarp;
+            s_next = nwarp * kRowBatch;
         }
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bnxt[i] = 0u;
         __syncthreads();
@@ -1541,14 +1550,40 @@ push_block_kernel(PushBlockParams p) {
         unsigned long long pc = 0, live_deg = 0;
         uint32_t sup = 0;
         float mx = 0.f, mn = 1.f;
-        // rows are claimed one at a time from a shared counter (row k = warp first), so a warp
-        // that meets a hub row does not hold the others at the round's barrier
-        for (uint32_t k = warp; k < nrows;) {
-            const uint32_t u = compact ? P[k] : k;
-            const uint32_t ub = __ldg(p.idx + u), ud = __ldg(p.idx + u + 1) - ub;
+        // Rows are claimed kRowBatch at a time from a shared counter (rows warp * kRowBatch .. first),
+        // so a warp that meets a hub row does not hold the others at the round's barrier.  The
+        // batch's row ids, offsets, first adjacency chunks and own values are loaded together, so
+        // their dependent loads are paid once per batch, not once per row.
+        for (uint32_t kb = warp * kRowBatch; kb < nrows;) {
+            uint32_t myu = 0, myb = 0, myd = 0;
+            if (lane < kRowBatch && kb + lane < nrows) {
+                myu = compact ? P[kb + lane] : kb + lane;
+                myb = __ldg(p.idx + myu);
+                myd = __ldg(p.idx + myu + 1) - myb;
+            }
+            uint32_t nb0[kRowBatch];
+            float own[kRowBatch];
+#pragma unroll
+            for (int i = 0; i < kRowBatch; ++i) {
+                const uint32_t ui = __shfl_sync(kFullMask, myu, i);
+                const uint32_t bi = __shfl_sync(kFullMask, myb, i);
+                const uint32_t di = __shfl_sync(kFullMask, myd, i);
+                const bool has = kb + uint32_t(i) < nrows;
+                nb0[i] = has && lane < di ? __ldg(p.adj + bi + lane) : 0u;
+                own[i] = has ? cur[size_t(ui) * S + lane] : 0.f;
+            }
+            unsigned nk = 0;
+            if (lane == 0) nk = atomicAdd(&s_next, uint32_t(kRowBatch));
+#pragma unroll
+            for (int i = 0; i < kRowBatch; ++i) {
+            if (kb + uint32_t(i) >= nrows) break;
+            const uint32_t u = __shfl_sync(kFullMask, myu, i);
+            const uint32_t ub = __shfl_sync(kFullMask, myb, i);
+            const uint32_t ud = __shfl_sync(kFullMask, myd, i);
             unsigned long long acc = 0;
             for (uint32_t c = 0; c < ud; c += 32) {
-                const uint32_t nb = c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u;
+                const uint32_t nb =
+                    c == 0 ? nb0[i] : (c + lane < ud ? __ldg(p.adj + ub + c + lane) : 0u);
                 // neighbours whose running columns are all zero add nothing: they are dropped, and
                 // the live ones compacted into lanes 0 .. popc(live) - 1 (the fixed-point sum does
                 // not depend on the order)
@@ -1559,27 +1594,21 @@ push_block_kernel(PushBlockParams p) {
                     lane < uint32_t(__popc(live)) ? __fns(live, 0, int(lane) + 1) : 0u;
                 const uint32_t packed = __shfl_sync(kFullMask, nb, nth);
                 const uint32_t kk = __popc(live);
-                uint32_t t = 0;
-                // eight independent 128-byte row loads in flight per step
-                for (; t + 8 <= kk; t += 8) {
+                // eight independent 128-byte row loads in flight per step; the last step's loads
+                // past kk are predicated off (a zero adds nothing), so a row's remainder costs one
+                // load latency, not one per neighbour
+                for (uint32_t t = 0; t < kk; t += 8) {
                     float x[8];
 #pragma unroll
-                    for (int h = 0; h < 8; ++h)
-                        x[h] = cur[size_t(__shfl_sync(kFullMask, packed, t + h)) * S + lane];
+                    for (int h = 0; h < 8; ++h) {
+                        const uint32_t v = __shfl_sync(kFullMask, packed, int((t + h) & 31u));
+                        x[h] = t + h < kk ? cur[size_t(v) * S + lane] : 0.f;
+                    }
 #pragma unroll
                     for (int h = 0; h < 8; ++h) acc += to_fixed(x[h]);
                 }
-                for (; t + 4 <= kk; t += 4) {
-                    const float x0 = cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane];
-                    const float x1 = cur[size_t(__shfl_sync(kFullMask, packed, t + 1)) * S + lane];
-                    const float x2 = cur[size_t(__shfl_sync(kFullMask, packed, t + 2)) * S + lane];
-                    const float x3 = cur[size_t(__shfl_sync(kFullMask, packed, t + 3)) * S + lane];
-                    acc += to_fixed(x0) + to_fixed(x1) + to_fixed(x2) + to_fixed(x3);
-                }
-                for (; t < kk; ++t)
-                    acc += to_fixed(cur[size_t(__shfl_sync(kFullMask, packed, t)) * S + lane]);
             }
-            float r = cur[size_t(u) * S + lane];
+            float r = own[i];
             if (run) {
                 r = acc ? from_fixed(acc, ud) : 0.f;
                 if (r > 0.f) {
@@ -1599,9 +1628,8 @@ push_block_kernel(PushBlockParams p) {
                 if (any_nz) Ln[atomicAdd(&s_ln, 1u)] = u;
             }
             nxt[size_t(u) * S + lane] = r;
-            unsigned nk = 0;
-            if (lane == 0) nk = atomicAdd(&s_next, 1u);
-            k = __shfl_sync(kFullMask, nk, 0);
+            }
+            kb = __shfl_sync(kFullMask, nk, 0);
         }
         if (run) {
             atomicAdd(s_picost + lane, pc);
@@ -2740,7 +2768,17 @@ source_kernel(Pack pk) {
         lap(5);
 
         // ---- 2-way bouquet walks (:241-391): four bouquets per warp, one per 8-lane group ----
-        if (nitems) {
+        if (nitems && p.walk_queue) {
+            // handed to walk_queue_kernel (the same walks, lanes and adds; more warps in flight)
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(p.walk_count, nitems);
+            base = __shfl_sync(kFullMask, base, 0);
+            for (uint32_t i = lane; i < nitems; i += 32) {
+                WalkItem w = items[i];
+                w.pad = entry;
+                p.walk_queue[base + i] = w;
+            }
+        } else if (nitems) {
             const uint32_t j = lane & 7, grp = lane >> 3;
             uint32_t next = 0;
             bool has = false, start = false, primary = true;
@@ -2871,6 +2909,132 @@ source_kernel(Pack pk) {
     }
     if (!SMEM && lane == 0) p0.wclean[gw] = (cleared && !dirty) ? 1 : 0;
     flush_stats(pk.g[last_gi == 0xffffffffu ? 0u : last_gi].stats);
+}
+
+// ---- walks of the block push's sources, as their own launch --------------------------------------
+// In PrePush mode the source kernel (a large kernel: 3 four-warp blocks per SM) leaves each
+// source's walking slots in a queue; this lean kernel walks them with many more warps in flight.
+// Everything a lane computes is what the source kernel's walk loop computes for the same item:
+// an 8-lane group takes one item, lane j walks the item's walks j, j + 8, ... in order over the
+// source's residual column, each hop's residual difference added to x in hop order, then the
+// group's eight x are summed in lane order into preds[slot] (src/aesc.h:241-391, 524-525).
+struct WalkQueueParams {
+    const uint32_t* idx;
+    const uint32_t* adj;
+    const uint32_t* rows;      // list entry -> source
+    const float* pre_cols;     // the block push's column blocks
+    const uint32_t* pre_final;
+    uint32_t list_base;        // first list entry of this wave
+    uint32_t n;
+    double* preds;
+    const WalkItem* items;
+    const unsigned* count;     // items in the queue
+    unsigned* claim;           // next item (zeroed before the launch)
+    unsigned long long* stats;
+};
+constexpr int kWalkThreads = 256;
+
+__global__ void __launch_bounds__(kWalkThreads, 5) walk_queue_kernel(const WalkQueueParams q) {
+    pdl_launch_dependents();
+    pdl_wait();  // the queue and the columns of this wave
+    const uint32_t lane = threadIdx.x & 31, j = lane & 7, grp = lane >> 3;
+    const uint32_t total = *q.count;
+    const uint32_t* __restrict__ idx = q.idx;
+    const uint32_t* __restrict__ adj = q.adj;
+    unsigned long long st_fb = 0;
+    bool has = false, start = false, primary = true, done = false;
+    WalkItem it{};
+    unsigned long long bi = 0;
+    uint32_t len = 0, step = 0, cur = 0, cur2 = 0, sec = 0, sec2 = 0, state = 0, src = 0;
+    float ds = 0.f;
+    const float* pvec = nullptr;
+    float x = 0.f, pa = 0.f, pb = 0.f;
+    bool pend = false;
+    while (true) {
+        // a group without an item claims the next one (items with nr = 0 are skipped)
+        if (!has && !done) {
+            unsigned my = 0;
+            if (j == 0) my = atomicAdd(q.claim, 1u);
+            my = __shfl_sync(0xffu << (grp * 8), my, int(grp * 8));
+            if (my >= total) {
+                done = true;
+            } else {
+                it = q.items[my];
+                if (it.nr) {
+                    has = true;
+                    start = true;
+                    bi = 0;
+                    x = 0.f;
+                    step = uint32_t(0xffffffffull / it.nr);
+                    src = __ldg(q.rows + it.pad);
+                    ds = float(__ldg(idx + src + 1) - __ldg(idx + src));
+                    const uint32_t slot = it.pad - q.list_base;
+                    const uint32_t cta = slot / kBlockCols, col = slot % kBlockCols;
+                    pvec = q.pre_cols +
+                           (size_t(cta) * 2 + (1u - q.pre_final[cta])) * size_t(q.n) * kBlockCols +
+                           size_t(col) * q.n;
+                }
+            }
+        }
+        if (!__any_sync(kFullMask, has || !done)) break;
+        if (has && start) {
+            cur = src;
+            cur2 = it.v;
+            sec = (uint32_t(bi) + j + 1u) * step;
+            sec2 = sec;
+            state = sec;
+            primary = true;
+            len = 0;
+            start = false;
+        }
+        const unsigned z = __ballot_sync(kFullMask, has && primary && (sec == 0u || sec2 == 0u));
+        if (has && primary && ((z >> (grp * 8)) & 0xffu)) {
+            primary = false;
+            if (j == 0) ++st_fb;
+        }
+        bool item_done = false;
+        if (has) {
+            const uint32_t b1 = __ldg(idx + cur), d1 = __ldg(idx + cur + 1) - b1;
+            const uint32_t b2 = __ldg(idx + cur2), d2 = __ldg(idx + cur2 + 1) - b2;
+            if (pend) x = radd(x, rsub(pa, pb));
+            uint32_t k1, k2;
+            if (primary) {
+                k1 = __umulhi(sec ^ fmix32(cur), d1);
+                k2 = __umulhi(sec2 ^ fmix32(cur2), d2);
+                sec *= d1;
+                sec2 *= d2;
+            } else {
+                const uint32_t r1 = splitmix32(state);
+                const uint32_t r2 = splitmix32(state);
+                k1 = r1 % d1;
+                k2 = r2 % d2;
+            }
+            cur = __ldg(adj + b1 + k1);
+            cur2 = __ldg(adj + b2 + k2);
+            pa = pvec[cur];
+            pb = pvec[cur2];
+            pend = true;
+            if (++len == it.len) {
+                bi += 8;
+                start = true;
+                item_done = bi >= it.nr;
+            }
+        }
+        if (__any_sync(kFullMask, item_done)) {
+            if (item_done && pend) {
+                x = radd(x, rsub(pa, pb));
+                pend = false;
+            }
+            double sum = 0;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) sum += double(__shfl_sync(kFullMask, x, int(grp * 8 + b)));
+            if (item_done && j == 0) q.preds[it.pos] += sum / (double(ds) * double(it.nr));
+            if (item_done) has = false;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) st_fb += __shfl_xor_sync(kFullMask, st_fb, o);
+    if (lane == 0) stat_add(q.stats, kStFallback, st_fb);
 }
 
 // ---- stage 3: symmetrise (src/aesc.h:532-550) -----------------------------------------------------
@@ -3125,7 +3289,7 @@ bool mixed_beyond_smem(uint64_t n) {
     return ((n * 4 + 15) & ~uint64_t(15)) + ((n + 15) & ~uint64_t(15)) + kAccBytes > uint64_t(112) * 1024;
 }
 void poll_push_hint(tgtp_graph* g);
-void post_push_hint(tgtp_graph* g, int key);
+void post_push_hint(tgtp_graph* g, int key, double eps);
 
 // JACOBI = mixed form (lane-parallel tau over Vec storage, frontier-parallel push).
 template <class Real, class Acc, bool JACOBI, class Vec>
@@ -3150,7 +3314,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     // block_ctas x kBlockCols listed sources (each wave has its own claim counter)
     // The block push gives the same bits as the per-warp push (fixed-point residual sums), so the
     // choice is only about speed: the handle's tuned layout, else TGTP_MIXED_BLOCK, else what the
-    // last completed mixed run on this graph measured (push_hint), else the block push for
+    // last completed mixed run on this graph at this epsilon measured (push_hint), else the block
+    // push for
     // vectors beyond shared memory at eps <= 0.01 (deep pushes: the block push was the faster one
     // on every such graph measured) and the per-warp push otherwise.
     const int key = form_key(cfg);
@@ -3158,9 +3323,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     bool block_mode = false;
     if (g->src_layout[key]) block_mode = JACOBI && (g->src_layout[key] & kLayoutBlock) != 0;
     else if (const char* e = std::getenv("TGTP_MIXED_BLOCK")) block_mode = JACOBI && std::atoi(e) != 0;
-    else if (g->push_hint[key]) block_mode = JACOBI && g->push_hint[key] == 2;
+    else if (g->push_hint[key] && g->push_hint_eps[key] == cfg.epsilon)
+        block_mode = JACOBI && g->push_hint[key] == 2;
     else block_mode = JACOBI && mixed_beyond_smem(n) && cfg.epsilon <= 0.01;
     g->last_key = key;
+    g->last_eps = cfg.epsilon;
     // CTAs of the block push: one per SM, within a budget for their residual blocks of 24 GB or
     // half the device memory free now (beside what the blocks already hold), whichever is larger
     // (TGTP_BLOCK_CTAS lowers the count, e.g. to exercise many waves on small graphs)
@@ -3375,6 +3542,8 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.adjd = g->adjd.as<uint2>();
     p.budget_ns = deadline_from_env();
     p.trace_nr = p.trace_ell = nullptr;
+    p.walk_queue = nullptr;
+    p.walk_count = nullptr;
     if (g->trace_on) {
         grow(g, g->trace, sizeof(uint32_t) * (m + n));
         TGTP_CUDA(cudaMemsetAsync(g->trace.ptr, 0, sizeof(uint32_t) * (m + n), s));
@@ -3490,6 +3659,27 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         bp.rows = sorted;
         p.rows = sorted;
         unsigned* claims = work + 4 + n + 1;
+        // the walks of each wave's sources: a queue of (slot, its source's list entry) items that
+        // walk_queue_kernel works through (a wave's sources hold at most m slots), and per wave a
+        // queue length and a claim counter
+        grow(g, g->walk_queue, sizeof(WalkItem) * (m + 1));
+        grow(g, g->walk_ctl, sizeof(unsigned) * 2 * (waves + 1));
+        unsigned* ctl = g->walk_ctl.as<unsigned>();
+        TGTP_CUDA(cudaMemsetAsync(ctl, 0, sizeof(unsigned) * 2 * (waves + 1), s));
+        p.walk_queue = g->walk_queue.as<WalkItem>();
+        WalkQueueParams wq;
+        wq.idx = p.idx;
+        wq.adj = p.adj;
+        wq.rows = sorted;
+        wq.pre_cols = bp.cols;
+        wq.pre_final = bp.final_buf;
+        wq.n = uint32_t(n);
+        wq.preds = reinterpret_cast<double*>(p.preds);
+        wq.items = p.walk_queue;
+        wq.stats = stats;
+        const int walk_per_sm =
+            blocks_per_sm(reinterpret_cast<const void*>(walk_queue_kernel), kWalkThreads, 0);
+        const unsigned walk_blocks = unsigned(g->num_sms) * unsigned(std::max(walk_per_sm, 1));
         for (uint32_t w = 0; w < waves; ++w) {
             bp.base = w * block_ctas * kBlockCols;
             {
@@ -3500,10 +3690,19 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             p.claim = claims + w;
             p.list_base = bp.base;
             p.list_cap = block_ctas * kBlockCols;
+            p.walk_count = ctl + 2 * w;
             pk.g[0] = p;
-            ScopedKernel k(g->prof, s, "source");
-            launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, pk);
-            TGTP_LAUNCH_CHECK("source_kernel");
+            {
+                ScopedKernel k(g->prof, s, "source");
+                launch(kern, unsigned(blocks), unsigned(threads), smem, s, true, pk);
+                TGTP_LAUNCH_CHECK("source_kernel");
+            }
+            wq.list_base = bp.base;
+            wq.count = ctl + 2 * w;
+            wq.claim = ctl + 2 * w + 1;
+            ScopedKernel k(g->prof, s, "walk_queue");
+            launch(walk_queue_kernel, walk_blocks, unsigned(kWalkThreads), size_t(0), s, true, wq);
+            TGTP_LAUNCH_CHECK("walk_queue_kernel");
         }
     }
     launch_finish<Real, Acc>(g, out);
@@ -3676,7 +3875,7 @@ void aesc_run(tgtp_graph* g, const tgtp_config& cfg, float* device_scores) {
             } else {
                 fail(TGTP_ERR_INVALID_ARGUMENT, "MIXED form stores eigenvectors as F32 or BF16");
             }
-            post_push_hint(g, form_key(cfg));
+            post_push_hint(g, form_key(cfg), cfg.epsilon);
             break;
         default:
             fail(TGTP_ERR_UNSUPPORTED, "unknown precision form");
@@ -3704,11 +3903,12 @@ namespace {
 // shared memory).  Measured on the sparse Chung-Lu graph (n = 25,860) at eps 0.05 / 0.01 / 0.005,
 // R-MAT (n = 143,522) at 0.05 / 0.01 and Chung-Lu (n = 199,772) at 0.05 / 0.01 / 0.005, the rule
 // picks the faster push every time (or one within 3 %).
-void learn_push_hint(tgtp_graph* g, int key, unsigned long long rounds,
+void learn_push_hint(tgtp_graph* g, int key, double eps, unsigned long long rounds,
                      unsigned long long traversals) {
     if (key < 2 || rounds == 0) return;
     const double per_round = double(traversals) / double(rounds);
     g->push_hint[key] = (mixed_beyond_smem(g->n) && per_round * 40.0 > double(g->m)) ? 2 : 1;
+    g->push_hint_eps[key] = eps;
 }
 
 // The counters of a completed mixed run copied to pinned memory (see tgtp_graph::hint_host), if
@@ -3726,14 +3926,14 @@ void poll_push_hint(tgtp_graph* g) {
         rounds += g->hint_host[size_t(c) * kStCount + kStPushRounds];
         trav += g->hint_host[size_t(c) * kStCount + kStPushTraversals];
     }
-    learn_push_hint(g, g->hint_key, rounds, trav);
+    learn_push_hint(g, g->hint_key, g->hint_eps, rounds, trav);
     g->hint_key = -1;
 }
 
 // After a mixed run on the handle's stream (not while capturing) on a graph whose vectors exceed
 // shared memory (smaller ones always push per warp): copy its counters to pinned memory and
 // record the event poll_push_hint looks at.
-void post_push_hint(tgtp_graph* g, int key) {
+void post_push_hint(tgtp_graph* g, int key, double eps) {
     if (!mixed_beyond_smem(g->n)) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     TGTP_CUDA(cudaStreamIsCapturing(g->stream, &cs));
@@ -3748,6 +3948,7 @@ void post_push_hint(tgtp_graph* g, int key) {
     TGTP_CUDA(cudaMemcpyAsync(g->hint_host, g->stats.ptr, bytes, cudaMemcpyDeviceToHost, g->stream));
     TGTP_CUDA(cudaEventRecord(g->hint_event, g->stream));
     g->hint_key = key;
+    g->hint_eps = eps;
 }
 
 }  // namespace
@@ -3767,7 +3968,7 @@ void aesc_read_stats(tgtp_graph* g, unsigned long long* st) {
     for (int i = 0; i < kStCount; ++i) st[i] = 0;
     for (int c = 0; c < kStStripes; ++c)
         for (int i = 0; i < kStCount; ++i) st[i] += stripes[size_t(c) * kStCount + i];
-    learn_push_hint(g, g->last_key, st[kStPushRounds], st[kStPushTraversals]);
+    learn_push_hint(g, g->last_key, g->last_eps, st[kStPushRounds], st[kStPushTraversals]);
 }
 
 int aesc_tune(tgtp_graph* g, const tgtp_config& cfg, float* device_scores, int trials) {

@@ -174,9 +174,11 @@ struct tgtp_graph {
     uint64_t wclean_sig[5] = {0, 0, 0, 0, 0};  // the scratch carving those marks belong to
     int batch_refs = 0;  // live batches whose CUDA graph points at this handle's buffers
     int last_key = -1;   // form of the last run (see form_key in aesc.cu)
+    double last_eps = 0;  // and its epsilon
     // mixed form, per vector storage: 2 when the last completed run's frontiers were large enough
     // for the multi-source block push to pay off, 1 when not, 0 unknown
     uint8_t push_hint[4] = {0, 0, 0, 0};
+    double push_hint_eps[4] = {0, 0, 0, 0};  // the epsilon each hint was measured at
     // each mixed run also copies its two push counters into pinned host memory behind an event;
     // the next run reads them there once the event has completed, so the hint is learned without
     // the caller reading the counters and without a synchronisation (hint_key: form of the copy
@@ -187,6 +189,7 @@ struct tgtp_graph {
     unsigned long long* hint_host = nullptr;
     cudaEvent_t hint_event = nullptr;
     int hint_key = -1;
+    double hint_eps = 0;
     bool has_f32 = false, has_f64 = false, has_bf16 = false;
 
     // run scratch
@@ -195,6 +198,7 @@ struct tgtp_graph {
     tgtp::DeviceBuffer block_cols, block_pre, block_final, block_keys, block_tmp;  // multi-source push
     tgtp::DeviceBuffer block_bits;   // the block push's row masks when they do not fit in smem
     tgtp::DeviceBuffer block_lists;  // the block push's row lists (four of n entries per CTA)
+    tgtp::DeviceBuffer walk_queue, walk_ctl;  // the block push's walk items; per wave length, claim
     // walk copy of the graph renumbered by degree (built on the first saba_count)
     tgtp::DeviceBuffer saba_info, saba_adj, saba_cnt;
     bool saba_ready = false;
