@@ -230,3 +230,45 @@ def test_mixed_and_fp64_differ_only_on_slots_next_to_a_pushed_row(cuda_device):
         assert np.all(~both_closed[dev > 1e-6])
         pushed_total += int((~both_closed).sum())
     assert pushed_total > 0
+
+
+@pytest.mark.parametrize("vec", ["f32", "bf16"])
+def test_block_push_walk_kernels_give_the_per_warp_walks_bits(cuda_device, monkeypatch, vec):
+    """After the block push the walks run in walk_queue_kernel (light items) and
+    heavy_walk_kernel (items of at least 512 walks of at most 32 hops, 32 bouquets at once): on
+    the sparse Chung-Lu graph (28,000 ids, 120,000 edges, exponent 2.1) at eps = 0.005, with both
+    kinds present (read from the run trace), the scores and walk counters equal the per-warp
+    push's, whose walks run in the source kernel."""
+    from tgtp_b200 import synth, workloads
+    from tgtp_b200.aesc import (AESC, AESCConfig, AESCGraph, PRECISION_MIXED, VEC_BF16,
+                                VEC_F32)
+
+    monkeypatch.setenv("TGTP_KERNEL_DEADLINE_S", "120")
+    sg = synth.chung_lu(28000, 120000, 2.1, 1)
+    idx, adj = sg.csr()
+    values, v32, _ = workloads._eigenpairs(sg, 128)
+    c = {"idx": idx, "adj": adj, "n": sg.n}
+    store = VEC_BF16 if vec == "bf16" else VEC_F32
+    g = AESCGraph.from_csr(idx, adj)
+    g.upload_eigens(values, v32, store)
+    got = {}
+    for block in ("0", "1"):
+        monkeypatch.setenv("TGTP_MIXED_BLOCK", block)
+        g.set_trace(True)
+        a = AESC(g, AESCConfig(0.005, precision=PRECISION_MIXED, vec_dtype=store))
+        s = a.tgtp()
+        st = a.stats()
+        nr, ell = g.read_trace()
+        taus = a.taus()[: len(c["adj"])].astype(np.int64)
+        g.set_trace(False)
+        got[block] = (s, {k: st[k] for k in ("push_rounds", "walk_edges", "walk_count", "walk_hops",
+                                             "fallback_bouquets")}, nr, ell, taus)
+    g.free()
+    assert np.array_equal(got["0"][0].view(np.uint32), got["1"][0].view(np.uint32))
+    assert got["0"][1] == got["1"][1]
+    nr, ell, taus = got["1"][2], got["1"][3], got["1"][4]
+    rows = np.repeat(np.arange(c["n"]), np.diff(c["idx"].astype(np.int64)))
+    walk_len = taus - ell[rows].astype(np.int64)
+    heavy = (nr >= 512) & (walk_len <= 32)
+    light = (nr > 0) & ~heavy
+    assert heavy.sum() > 0 and light.sum() > 0, (int(heavy.sum()), int(light.sum()))

@@ -980,9 +980,12 @@ struct SourceParams {
     uint32_t* trace_nr;
     uint32_t* trace_ell;
     // PrePush mode: when set, a source's walking slots (with their nr) are appended to this queue
-    // (walk_count counts them) and walk_queue_kernel walks them, instead of the warp here
+    // instead of being walked by the warp here: light items from the front (walk_count[0] counts
+    // them; walk_queue_kernel walks them), heavy ones (many walks of few hops) from the back
+    // (walk_count[2]; heavy_walk_kernel).  walk_cap entries.
     WalkItem* walk_queue;
     unsigned* walk_count;
+    uint32_t walk_cap;
 };
 
 // The source kernel's parameters: one graph (N = 1), or up to N graphs whose listed rows one
@@ -1254,6 +1257,10 @@ __device__ __forceinline__ void seg_maxmin(uint32_t seg, Real& mx, Real& mn) {
 // column holds its source's final residual vector; the edge bound, chi and walks of those sources
 // then run in source_kernel (PrePush mode), which copies the column into its own residual vector.
 constexpr int kBlockCols = 32;
+// Walk items of the block push's sources with at least kHeavyNr walks of at most kHeavyLen hops
+// go to heavy_walk_kernel, which walks 32 of their bouquets at once instead of one after another.
+constexpr unsigned long long kHeavyNr = 512;
+constexpr uint32_t kHeavyLen = 32;
 // rows a warp of push_block_kernel claims at a time (their dependent loads are issued together).
 // Measured on three graphs (n = 25,860 / 143,522 / 199,772): 1 row is 3-6 % faster than the plain
 // loop (the row's own value and first adjacency chunk are requested before its neighbours are
@@ -2769,14 +2776,31 @@ source_kernel(Pack pk) {
 
         // ---- 2-way bouquet walks (:241-391): four bouquets per warp, one per 8-lane group ----
         if (nitems && p.walk_queue) {
-            // handed to walk_queue_kernel (the same walks, lanes and adds; more warps in flight)
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(p.walk_count, nitems);
-            base = __shfl_sync(kFullMask, base, 0);
-            for (uint32_t i = lane; i < nitems; i += 32) {
-                WalkItem w = items[i];
-                w.pad = entry;
-                p.walk_queue[base + i] = w;
+            // handed to walk_queue_kernel / heavy_walk_kernel (the same walks, lanes and adds;
+            // more warps in flight)
+            for (uint32_t c = 0; c < nitems; c += 32) {
+                const uint32_t i = c + lane;
+                const bool has = i < nitems;
+                WalkItem w{};
+                bool heavy = false;
+                if (has) {
+                    w = items[i];
+                    w.pad = entry;
+                    heavy = w.nr >= kHeavyNr && w.len <= kHeavyLen;
+                }
+                const unsigned bh = __ballot_sync(kFullMask, has && heavy);
+                const unsigned bl = __ballot_sync(kFullMask, has && !heavy);
+                unsigned lb = 0, hb = 0;
+                if (lane == 0) {
+                    if (bl) lb = atomicAdd(p.walk_count, unsigned(__popc(bl)));
+                    if (bh) hb = atomicAdd(p.walk_count + 2, unsigned(__popc(bh)));
+                }
+                lb = __shfl_sync(kFullMask, lb, 0);
+                hb = __shfl_sync(kFullMask, hb, 0);
+                if (has) {
+                    if (heavy) p.walk_queue[p.walk_cap - 1u - (hb + __popc(bh & lt))] = w;
+                    else p.walk_queue[lb + __popc(bl & lt)] = w;
+                }
             }
         } else if (nitems) {
             const uint32_t j = lane & 7, grp = lane >> 3;
@@ -3030,6 +3054,104 @@ __global__ void __launch_bounds__(kWalkThreads, 5) walk_queue_kernel(const WalkQ
             for (int b = 0; b < 8; ++b) sum += double(__shfl_sync(kFullMask, x, int(grp * 8 + b)));
             if (item_done && j == 0) q.preds[it.pos] += sum / (double(ds) * double(it.nr));
             if (item_done) has = false;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) st_fb += __shfl_xor_sync(kFullMask, st_fb, o);
+    if (lane == 0) stat_add(q.stats, kStFallback, st_fb);
+}
+
+// Heavy walk items (at least kHeavyNr walks of at most kHeavyLen hops; a few per wave, which would
+// otherwise hold a whole wave for one 8-lane group walking them one bouquet after another; on large
+// graphs low-degree sources reach 10^6 walks and more).  One 1,024-thread block per item walks 128
+// bouquets at once: thread 8r + j walks walk bi + j of bouquet r (bi = the bouquet's first walk)
+// and keeps each hop's residual difference in shared memory; then thread j (the item's lane j)
+// adds its walks' differences to x in walk order and hop order -- the adds, values and order of
+// walk_queue_kernel's lane j -- and the eight x are summed as there.
+constexpr int kHeavyThreads = 1024;
+constexpr size_t kHeavySmem = sizeof(float) * kHeavyThreads * (kHeavyLen + 1);
+
+__global__ void __launch_bounds__(kHeavyThreads) heavy_walk_kernel(const WalkQueueParams q,
+                                                                   uint32_t cap) {
+    extern __shared__ float s_heavy[];
+    float (*s_d)[kHeavyLen + 1] = reinterpret_cast<float (*)[kHeavyLen + 1]>(s_heavy);
+    __shared__ unsigned s_item;
+    pdl_launch_dependents();
+    pdl_wait();
+    const uint32_t tid = threadIdx.x, lane = tid & 31, j = tid & 7, grp = lane >> 3;
+    const uint32_t r = tid >> 3;  // bouquet of the chunk
+    const uint32_t total = *q.count;
+    const uint32_t* __restrict__ idx = q.idx;
+    const uint32_t* __restrict__ adj = q.adj;
+    unsigned long long st_fb = 0;
+    while (true) {
+        if (tid == 0) s_item = atomicAdd(q.claim, 1u);
+        __syncthreads();
+        const unsigned my = s_item;
+        __syncthreads();
+        if (my >= total) break;
+        const WalkItem it = q.items[cap - 1u - my];
+        const uint32_t src = __ldg(q.rows + it.pad);
+        const float ds = float(__ldg(idx + src + 1) - __ldg(idx + src));
+        const uint32_t slot = it.pad - q.list_base;
+        const uint32_t cta = slot / kBlockCols, col = slot % kBlockCols;
+        const float* pvec = q.pre_cols +
+                            (size_t(cta) * 2 + (1u - q.pre_final[cta])) * size_t(q.n) * kBlockCols +
+                            size_t(col) * q.n;
+        const uint32_t step = uint32_t(0xffffffffull / it.nr);
+        const uint32_t L = it.len;
+        float x = 0.f;  // threads 0..7
+        for (unsigned long long c0 = 0; c0 < it.nr; c0 += kHeavyThreads) {
+            const unsigned long long bi = c0 + 8ull * r;
+            const bool active = bi < it.nr;
+            uint32_t cur = src, cur2 = it.v;
+            uint32_t sec = (uint32_t(bi) + j + 1u) * step, sec2 = sec, state = sec;
+            bool primary = true;
+            // each hop's residual pair is stored one hop later, after the next hop's row offsets
+            // are requested, so the residual loads stay off the walk's chain of dependent loads
+            float pa = 0.f, pb = 0.f;
+            for (uint32_t h = 0; h < L; ++h) {
+                const unsigned z =
+                    __ballot_sync(kFullMask, active && primary && (sec == 0u || sec2 == 0u));
+                if (active && primary && ((z >> (grp * 8)) & 0xffu)) {
+                    primary = false;
+                    if (j == 0) ++st_fb;
+                }
+                if (active) {
+                    const uint32_t b1 = __ldg(idx + cur), d1 = __ldg(idx + cur + 1) - b1;
+                    const uint32_t b2 = __ldg(idx + cur2), d2 = __ldg(idx + cur2 + 1) - b2;
+                    if (h > 0) s_d[tid][h - 1] = rsub(pa, pb);
+                    uint32_t k1, k2;
+                    if (primary) {
+                        k1 = __umulhi(sec ^ fmix32(cur), d1);
+                        k2 = __umulhi(sec2 ^ fmix32(cur2), d2);
+                        sec *= d1;
+                        sec2 *= d2;
+                    } else {
+                        const uint32_t r1 = splitmix32(state);
+                        const uint32_t r2 = splitmix32(state);
+                        k1 = r1 % d1;
+                        k2 = r2 % d2;
+                    }
+                    cur = __ldg(adj + b1 + k1);
+                    cur2 = __ldg(adj + b2 + k2);
+                    pa = pvec[cur];
+                    pb = pvec[cur2];
+                }
+            }
+            if (active && L > 0) s_d[tid][L - 1] = rsub(pa, pb);
+            __syncthreads();
+            if (tid < 8) {
+                for (uint32_t b = 0; b < kHeavyThreads / 8 && c0 + 8ull * b < it.nr; ++b)
+                    for (uint32_t h = 0; h < L; ++h) x = radd(x, s_d[8 * b + tid][h]);
+            }
+            __syncthreads();
+        }
+        if (tid < 32) {
+            double sum = 0;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) sum += double(__shfl_sync(kFullMask, x, b));
+            if (tid == 0) q.preds[it.pos] += sum / (double(ds) * double(it.nr));
         }
     }
 #pragma unroll
@@ -3544,6 +3666,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
     p.trace_nr = p.trace_ell = nullptr;
     p.walk_queue = nullptr;
     p.walk_count = nullptr;
+    p.walk_cap = 0;
     if (g->trace_on) {
         grow(g, g->trace, sizeof(uint32_t) * (m + n));
         TGTP_CUDA(cudaMemsetAsync(g->trace.ptr, 0, sizeof(uint32_t) * (m + n), s));
@@ -3663,10 +3786,11 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         // walk_queue_kernel works through (a wave's sources hold at most m slots), and per wave a
         // queue length and a claim counter
         grow(g, g->walk_queue, sizeof(WalkItem) * (m + 1));
-        grow(g, g->walk_ctl, sizeof(unsigned) * 2 * (waves + 1));
+        grow(g, g->walk_ctl, sizeof(unsigned) * 4 * (waves + 1));
         unsigned* ctl = g->walk_ctl.as<unsigned>();
-        TGTP_CUDA(cudaMemsetAsync(ctl, 0, sizeof(unsigned) * 2 * (waves + 1), s));
+        TGTP_CUDA(cudaMemsetAsync(ctl, 0, sizeof(unsigned) * 4 * (waves + 1), s));
         p.walk_queue = g->walk_queue.as<WalkItem>();
+        p.walk_cap = uint32_t(m + 1);
         WalkQueueParams wq;
         wq.idx = p.idx;
         wq.adj = p.adj;
@@ -3680,6 +3804,9 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
         const int walk_per_sm =
             blocks_per_sm(reinterpret_cast<const void*>(walk_queue_kernel), kWalkThreads, 0);
         const unsigned walk_blocks = unsigned(g->num_sms) * unsigned(std::max(walk_per_sm, 1));
+        const int heavy_per_sm = blocks_per_sm(reinterpret_cast<const void*>(heavy_walk_kernel),
+                                               kHeavyThreads, kHeavySmem);
+        const unsigned heavy_blocks = unsigned(g->num_sms) * unsigned(std::max(heavy_per_sm, 1));
         for (uint32_t w = 0; w < waves; ++w) {
             bp.base = w * block_ctas * kBlockCols;
             {
@@ -3690,7 +3817,7 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
             p.claim = claims + w;
             p.list_base = bp.base;
             p.list_cap = block_ctas * kBlockCols;
-            p.walk_count = ctl + 2 * w;
+            p.walk_count = ctl + 4 * w;
             pk.g[0] = p;
             {
                 ScopedKernel k(g->prof, s, "source");
@@ -3698,11 +3825,20 @@ void run_form(tgtp_graph* g, const tgtp_config& cfg, float* out) {
                 TGTP_LAUNCH_CHECK("source_kernel");
             }
             wq.list_base = bp.base;
-            wq.count = ctl + 2 * w;
-            wq.claim = ctl + 2 * w + 1;
-            ScopedKernel k(g->prof, s, "walk_queue");
-            launch(walk_queue_kernel, walk_blocks, unsigned(kWalkThreads), size_t(0), s, true, wq);
-            TGTP_LAUNCH_CHECK("walk_queue_kernel");
+            wq.count = ctl + 4 * w;
+            wq.claim = ctl + 4 * w + 1;
+            {
+                ScopedKernel k(g->prof, s, "walk_queue");
+                launch(walk_queue_kernel, walk_blocks, unsigned(kWalkThreads), size_t(0), s, true, wq);
+                TGTP_LAUNCH_CHECK("walk_queue_kernel");
+            }
+            WalkQueueParams wh = wq;
+            wh.count = ctl + 4 * w + 2;
+            wh.claim = ctl + 4 * w + 3;
+            ScopedKernel k(g->prof, s, "heavy_walk");
+            launch(heavy_walk_kernel, heavy_blocks, unsigned(kHeavyThreads), kHeavySmem, s, true, wh,
+                   uint32_t(m + 1));
+            TGTP_LAUNCH_CHECK("heavy_walk_kernel");
         }
     }
     launch_finish<Real, Acc>(g, out);
