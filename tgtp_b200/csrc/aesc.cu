@@ -1148,8 +1148,10 @@ __device__ void kth_largest(const uint32_t* q, uint32_t qs, const Real* pvec, in
 // leaves, whose positive entries are exactly the final frontier, in vertex order): the same
 // selection without the frontier list, as contiguous pipelined loads.
 template <class Real>
-__device__ void kth_largest_col(const Real* col, uint32_t n, int rg, Real& t, int& n_eq_taken) {
+__device__ void kth_largest_col(const Real* col, uint32_t n, int rg, Real& t, int& n_eq_taken,
+                                uint32_t* cand = nullptr, uint32_t* ncand = nullptr) {
     const uint32_t lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     auto load_v = [&](uint32_t i0, Real* r) {
 #pragma unroll
         for (int b = 0; b < kB; ++b) {
@@ -1162,10 +1164,21 @@ __device__ void kth_largest_col(const Real* col, uint32_t n, int rg, Real& t, in
         Real L[kTopK];
 #pragma unroll
         for (int j = 0; j < kTopK; ++j) L[j] = Real(-INFINITY);
-        pipelined<Real>(n, load_v, [&](uint32_t, const Real* r) {
+        // With cand: every positive entry that reaches its lane's top kTopK so far (x >= the
+        // lane's current kTopK-th value) is listed, in index order.  An entry not listed had
+        // kTopK >= rg larger ones before it, so it is below the rg-th largest value; every entry
+        // at or above that value has fewer than rg larger ones and is listed.
+        uint32_t nc = 0;
+        pipelined<Real>(n, load_v, [&](uint32_t i0, const Real* r) {
 #pragma unroll
             for (int b = 0; b < kB; ++b) {
                 const Real x = r[b];
+                if (cand) {
+                    const bool rec = x > Real(-INFINITY) && x >= L[kTopK - 1];
+                    const unsigned bal = __ballot_sync(kFullMask, rec);
+                    if (rec) cand[nc + __popc(bal & below)] = i0 + 32 * b + lane;
+                    nc += __popc(bal);
+                }
                 if (x > L[kTopK - 1]) {
 #pragma unroll
                     for (int j = kTopK - 1; j > 0; --j) {
@@ -1191,6 +1204,7 @@ __device__ void kth_largest_col(const Real* col, uint32_t n, int rg, Real& t, in
         }
         t = last;
         n_eq_taken = run;
+        if (ncand) *ncand = nc;
         return;
     }
     Real thr = Real(INFINITY);
@@ -2525,8 +2539,40 @@ source_kernel(Pack pk) {
             if (p.gamma < nnz && from_col) {
                 Real t;
                 int need_eq;
-                kth_largest_col<Real>(pvec, n, rg, t, need_eq);
+                // top-gamma threshold and, for gamma <= kTopK, the list of the only entries that
+                // can reach it (in index order, into q, free in this mode): the set is then taken
+                // from that list instead of a second pass over the column
+                const bool use_cand = rg <= kTopK;
+                uint32_t nc = 0;
+                kth_largest_col<Real>(pvec, n, rg, t, need_eq, use_cand ? q : nullptr, &nc);
                 int taken_eq = 0;
+                __syncwarp();
+                if (use_cand) {
+                    pipelined<uint32_t>(nc,
+                        [&](uint32_t i0, uint32_t* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const uint32_t i = i0 + 32 * b + lane;
+                                r[b] = i < nc ? q[i] : NONE;
+                            }
+                        },
+                        [&](uint32_t, const uint32_t* r) {
+#pragma unroll
+                            for (int b = 0; b < kB; ++b) {
+                                const bool valid = r[b] != NONE;
+                                const Real v = valid ? pvec[r[b]] : Real(0);
+                                const Real x = v > Real(0) ? v : Real(-INFINITY);
+                                const bool gt = valid && x > t, eq = valid && x == t;
+                                const unsigned be = __ballot_sync(kFullMask, eq);
+                                const bool take_eq = eq && taken_eq + __popc(be & lt) < need_eq;
+                                const bool take = (gt || take_eq) && sc < rg;
+                                const unsigned bt = __ballot_sync(kFullMask, take);
+                                if (take) set[sc + __popc(bt & lt)] = r[b];
+                                sc += __popc(bt);
+                                taken_eq += __popc(__ballot_sync(kFullMask, take_eq));
+                            }
+                        });
+                } else
                 pipelined<Real>(n,
                     [&](uint32_t i0, Real* r) {
 #pragma unroll
