@@ -392,8 +392,12 @@ void graph_prepare(tgtp_graph* g) {
     g->row_of.reserve(sizeof(uint32_t) * (m + 1));
     g->rev.reserve(sizeof(uint32_t) * (m + 1));
     g->sym_src.reserve(sizeof(uint32_t) * (m + 1));
-    // first the maps that read neighbour ids only as values, the checks, the forward counts
-    DeviceBuffer cnt, lbp;
+    // first the maps that read neighbour ids only as values, the checks, the forward counts.  The
+    // per-row scratch is the handle's (released with it), so returning does not wait for the
+    // kernels after the checks: the caller's next call on the stream overlaps them (e.g. the
+    // eigenvector copy)
+    DeviceBuffer& cnt = g->prep_cnt;
+    DeviceBuffer& lbp = g->prep_lbp;
     cnt.reserve(sizeof(uint32_t) * (n + 8));
     lbp.reserve(sizeof(uint32_t) * (n + 1));
     auto* c = cnt.as<uint32_t>();
@@ -445,7 +449,6 @@ void graph_prepare(tgtp_graph* g) {
             adj, g->row_of.as<uint32_t>(), g->rev.as<uint32_t>(), m, c, lbp.as<uint32_t>(),
             g->forward.as<uint32_t>(), g->fedge.as<uint4>());
     TGTP_LAUNCH_CHECK("forward_fill_kernel");
-    // the temporaries go back to the cache when this returns (their release waits for the device)
 }
 
 }  // namespace tgtp

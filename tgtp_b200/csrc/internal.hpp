@@ -158,6 +158,7 @@ struct tgtp_graph {
     tgtp::DeviceBuffer forward;  // slots with v >= u, in CSR order
     tgtp::DeviceBuffer fedge;    // per forward slot: (u, v, slot, reverse slot)
     tgtp::DeviceBuffer adjd;     // slot -> (neighbour, neighbour's degree)
+    tgtp::DeviceBuffer prep_cnt, prep_lbp;  // graph_prepare's per-row forward counts and bounds
 
     // eigenpairs
     uint32_t omega = 0;
