@@ -326,3 +326,17 @@ def test_mt_walk_oracle_matches_the_reference_walks(tmp_path, oracle_lib, tgtp_l
     n, m, visits, checksum = (int(x) for x in r.stdout.split())
     assert (n, m) == (g.n, len(adj)) and visits == int(got.sum())
     assert checksum == int((got * np.arange(1, n + 1, dtype=np.uint64)).sum())
+
+
+@pytest.mark.parametrize("simd", [False, True])
+def test_mt_walk_oracle_does_not_depend_on_its_thread_count(oracle_lib, simd):
+    """Every source reseeds its own generator, so the counters are the same however the sources are
+    spread over threads (the reference's OpenMP loop relies on the same property)."""
+    from tgtp_b200 import synth
+
+    g = synth.rmat(12, 8, 0.57, 0.19, 0.19, 5)
+    idx, adj = g.csr()
+    one = oracle_lib.mt_walks(idx, adj, 7, 24, simd=simd, threads=1)
+    four = oracle_lib.mt_walks(idx, adj, 7, 24, simd=simd, threads=4)
+    assert np.array_equal(one, four)
+    assert int(one.sum()) == int((np.diff(idx.astype(np.int64)) > 0).sum()) * 24 * 7
