@@ -193,7 +193,7 @@ tgtp_status saba_count_device(tgtp_graph* g, uint32_t depth, uint32_t n_walks,
 
 /* Times the walk layouts for this graph and walk configuration and keeps the fastest on the handle
  * for later saba_count calls: 1, 2 or 4 walkers per lane (4, 8 or 16 eight-lane bouquets per warp)
- * over the degree-renumbered walk copy, plain (with none, 2,048 or 3,072 of the highest-degree row
+ * over the degree-renumbered walk copy, plain (with none, 3,072 or 4,096 of the highest-degree row
  * records held in shared memory) or with the next row's record inlined in each slot.  `trials`
  * timed runs each after a warm-up.  *choice (may be NULL) receives the pick: low byte = walkers per
  * lane, 0x100 = inlined copy, bits 12-14 = c for 1,024 x c shared row records.

@@ -157,16 +157,27 @@ __global__ void saba_scatter_kernel(const uint32_t* __restrict__ cnt, const uint
 // The row records of the first `hot_rec` numbers (the highest degrees, which take most hops: on
 // R-MAT scale 18 the top 2,048 / 4,096 vertices hold 38 % / 52 % of the degree mass) are copied
 // into shared memory, so a hop that lands there makes one random L1/L2 load instead of two.
-// Shared memory: hot_rec 16-byte records, then `hot` 4-byte counters (hot_rec <= hot <= n).
+// Shared memory: hot_rec 12-byte records (three arrays), then `hot` 4-byte counters
+// (hot_rec <= hot <= n).
 template <int WPL>
 __global__ void __launch_bounds__(kSabaThreads)
 saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict__ adjp,
                       uint32_t depth, uint32_t bouquets_per_src, uint32_t grid_step,
                       uint64_t total_bouquets, uint32_t* __restrict__ cnt, uint32_t hot,
                       uint32_t hot_rec, unsigned long long* __restrict__ fallback_total) {
-    extern __shared__ uint4 s_rec[];
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_rec + hot_rec);
-    for (uint32_t i = threadIdx.x; i < hot_rec; i += blockDim.x) s_rec[i] = __ldg(info + i);
+    // the records as three arrays (row start, degree, original id: 12 bytes a vertex), then the
+    // counters
+    extern __shared__ uint32_t s_words[];
+    uint32_t* s_beg = s_words;
+    uint32_t* s_deg = s_beg + hot_rec;
+    uint32_t* s_org = s_deg + hot_rec;
+    uint32_t* s_cnt = s_org + hot_rec;
+    for (uint32_t i = threadIdx.x; i < hot_rec; i += blockDim.x) {
+        const uint4 r = __ldg(info + i);
+        s_beg[i] = r.x;
+        s_deg[i] = r.y;
+        s_org[i] = r.z;
+    }
     for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
 
@@ -229,12 +240,16 @@ saba_walk_perm_kernel(const uint4* __restrict__ info, const uint32_t* __restrict
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 if (active[w]) {
-                    uint4 r;
-                    if (nxt[w] < hot_rec) r = s_rec[nxt[w]];
-                    else r = __ldg(info + nxt[w]);
-                    beg[w] = r.x;
-                    d[w] = r.y;
-                    orig[w] = r.z;
+                    if (nxt[w] < hot_rec) {
+                        beg[w] = s_beg[nxt[w]];
+                        d[w] = s_deg[nxt[w]];
+                        orig[w] = s_org[nxt[w]];
+                    } else {
+                        const uint4 r = __ldg(info + nxt[w]);
+                        beg[w] = r.x;
+                        d[w] = r.y;
+                        orig[w] = r.z;
+                    }
                     if (nxt[w] < hot) atomicAdd(s_cnt + nxt[w], 1u);
                     else atomicAdd(cnt + nxt[w], 1u);
                 }
@@ -455,17 +470,18 @@ bool saba_use_inline(const tgtp_graph* g) {
 }
 
 // Row records of the plain walk copy kept in shared memory (the highest-degree numbers): the tuned
-// choice (saba_tune: 1,024 x bits 12-14 of the choice), else TGTP_SABA_HOT_REC, else 3,072.
-// Shared memory and L1 share 256 KB per SM: with the default 12,288 counters, 3,072 records make a
-// 96 KB block, two of which leave 60 KB of L1 for the walk copy; on R-MAT scale 18 (D 5 / 10 / 15,
-// W 2,048 / 16,384) that measured 1.09-1.11x the 2,048-record block and 1.06-1.28x no records
-// with one walker per lane, while any split that left under 32 KB of L1 (three 72 KB blocks, or
-// two of 104 KB) lost about a third.
+// choice (saba_tune: 1,024 x bits 12-14 of the choice), else TGTP_SABA_HOT_REC, else 4,096.
+// Shared memory and L1 share 256 KB per SM: with the default 12,288 counters, 4,096 records of
+// 12 bytes make a 96 KB block, two of which leave 60 KB of L1 for the walk copy.  On R-MAT scale 18
+// (D 5 / 10 / 15, W 2,048 / 16,384): 3,072 records (as 16-byte records, the same block size)
+// measured 1.09-1.11x 2,048 and 1.06-1.28x no records with one walker per lane; 4,096 12-byte
+// records 1.03-1.04x 3,072; any split that left under 32 KB of L1 (three 72 KB blocks, or two of
+// 102-104 KB) lost about a third.
 uint32_t saba_hot_records(const tgtp_graph* g) {
     if (g->saba_choice) return 1024u * ((g->saba_choice >> 12) & 7u);
     if (const char* e = std::getenv("TGTP_SABA_HOT_REC"))
         return uint32_t(std::max(0, std::min(std::atoi(e), 8192)));
-    return 3072u;
+    return 4096u;
 }
 
 void saba_prepare_inline(tgtp_graph* g) {
@@ -492,7 +508,7 @@ void saba_launch(tgtp_graph* g, uint32_t depth, uint32_t bps, uint32_t grid_step
     const uint32_t hot = uint32_t(g->n < cap ? g->n : cap);
     const bool inl = saba_use_inline(g);
     const uint32_t hot_rec = inl ? 0u : std::min(hot, saba_hot_records(g));
-    const size_t smem = sizeof(uint32_t) * hot + sizeof(uint4) * hot_rec;
+    const size_t smem = sizeof(uint32_t) * (hot + 3 * size_t(hot_rec));
     if (inl) saba_prepare_inline(g);
     const void* kern = inl ? reinterpret_cast<const void*>(saba_walk_inline_kernel<WPL>)
                            : reinterpret_cast<const void*>(saba_walk_perm_kernel<WPL>);
@@ -554,8 +570,8 @@ int saba_tune(tgtp_graph* g, uint32_t depth, uint32_t n_walks, int trials) {
     std::vector<uint16_t> cand;
     for (int wpl : {1, 2, 4}) {
         if (saba_inline_fits(g)) cand.push_back(uint16_t(0x100 | wpl));
-        // plain copy: no hot records, or 2,048 / 3,072 of them in shared memory
-        for (int code : {0, 2, 3}) cand.push_back(uint16_t((code << 12) | wpl));
+        // plain copy: no hot records, or 3,072 / 4,096 of them in shared memory
+        for (int code : {0, 3, 4}) cand.push_back(uint16_t((code << 12) | wpl));
     }
     g->counters.reserve(sizeof(uint32_t) * (g->n + 1));
     auto* c = g->counters.as<uint32_t>();
