@@ -326,3 +326,24 @@ def test_run_trace_adds_up_to_the_run_counters(cuda_device, config1_inputs, form
     assert np.all(ell[rows[nr > 0]] >= 1)
     assert np.all(nr[nr > 0] % 8 == 0)
     g.free()
+
+
+def test_run_trace_is_refused_before_a_traced_run(cuda_device, config1_inputs):
+    """read_trace without a traced run on the handle (trace off, or on but no run since) is an
+    invalid-argument status, not stale data."""
+    from tgtp_b200.aesc import AESC, AESCConfig, AESCGraph, TgtpError, VEC_F32
+
+    c = config1_inputs
+    g = AESCGraph.from_csr(c["idx"], c["adj"])
+    g.upload_eigens(c["values"], c["v32"], VEC_F32)
+    with pytest.raises(TgtpError) as e:
+        g.read_trace()
+    assert e.value.status == 1
+    AESC(g, AESCConfig(0.05)).tgtp()
+    g.set_trace(True)
+    with pytest.raises(TgtpError):
+        g.read_trace()
+    AESC(g, AESCConfig(0.05)).tgtp()
+    nr, ell = g.read_trace()
+    assert nr.shape == (len(c["adj"]),) and ell.shape == (c["n"],)
+    g.free()
