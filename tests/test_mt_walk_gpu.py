@@ -83,3 +83,28 @@ def test_mt_walk_runners_print_the_oracle_sums(cuda_device, oracle_lib, tmp_path
     assert [ln.split(" ")[0] for ln in lines] == [
         "variant", "dataset", "depth", "n_walks", "threads", "n_vertices", "n_edges", "t_load_s",
         "t_rw_s", "total_s", "total_walks", "walks_per_sec", "visit_count", "checksum"]
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_mt_walks_match_the_committed_reference_counters(cuda_device, case):
+    """The GPU walks against tests/golden/mt_walks.json (the reference's own walk routines, run by
+    tests/golden/make_mt_walks.py): every counter, by SHA-256 of the array."""
+    import json
+
+    from conftest import GOLDEN
+    from make_mt_walks import graph
+    from make_saba_rmat18 import graph_fingerprint, sha256_u32
+
+    from tgtp_b200.aesc import AESCGraph, mt_walk_count
+
+    with open(os.path.join(GOLDEN, "mt_walks.json")) as f:
+        c = json.load(f)["cases"][case]
+    g = graph(c["graph"])
+    idx, adj = g.csr()
+    assert graph_fingerprint(idx, adj) == c["graph_fingerprint"]
+    dg = AESCGraph.from_csr(idx, adj)
+    counts, visits, checksum = mt_walk_count(dg, c["depth"], c["n_walks"], simd=c["simd"])
+    dg.free()
+    assert (visits, checksum, int(counts.max())) == (c["visit_count"], c["checksum"],
+                                                    c["max_counter"])
+    assert sha256_u32(counts) == c["counters_sha256"]

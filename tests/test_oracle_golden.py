@@ -340,3 +340,28 @@ def test_mt_walk_oracle_does_not_depend_on_its_thread_count(oracle_lib, simd):
     four = oracle_lib.mt_walks(idx, adj, 7, 24, simd=simd, threads=4)
     assert np.array_equal(one, four)
     assert int(one.sum()) == int((np.diff(idx.astype(np.int64)) > 0).sum()) * 24 * 7
+
+
+def _mt_fixture():
+    import json
+
+    with open(os.path.join(GOLDEN, "mt_walks.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_mt_walk_oracle_matches_the_committed_reference_counters(oracle_lib, case):
+    """The oracle's MT19937 walks against tests/golden/mt_walks.json (the reference's own walk
+    routines, run by tests/golden/make_mt_walks.py): every counter, by SHA-256 of the array, so the
+    pin holds where the reference binaries are not built."""
+    from make_mt_walks import graph
+    from make_saba_rmat18 import graph_fingerprint, sha256_u32
+
+    c = _mt_fixture()["cases"][case]
+    g = graph(c["graph"])
+    idx, adj = g.csr()
+    assert graph_fingerprint(idx, adj) == c["graph_fingerprint"]
+    got = oracle_lib.mt_walks(idx, adj, c["depth"], c["n_walks"], simd=c["simd"])
+    assert int(got.sum()) == c["visit_count"]
+    assert int((got * np.arange(1, g.n + 1, dtype=np.uint64)).sum()) == c["checksum"]
+    assert sha256_u32(got.astype(np.uint32)) == c["counters_sha256"]
